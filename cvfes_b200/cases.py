@@ -1,0 +1,124 @@
+"""Synthetic wall workloads: structured tubes with seeded GMRF material.
+
+No public dataset exists for this path; every workload is generated.  The
+tube sizes, material law and load follow the workload definitions:
+
+``tube64x128``   straight tube r=0.3 cm, L=3 cm, 64 x 128 nodes, 8 samples, dt 2e-6, 400 steps, FP64
+``tube256x1024`` same tube refined to 256 x 1024 nodes, 512 samples, dt 5e-7, 2000 steps
+``batched64``    64 tubes, r in [0.15,0.6], L in [1,6], nc in {32..256}, na in [64,1024],
+                 S in {16..256}, per-tube CFL dt, 1000 steps
+``adjoint64``    tube64x128 mesh, 64 samples, 500 steps, 512 observation nodes
+``stenosed512x2048`` stenosed tube L=5 cm, 512 x 2048 nodes, 128 samples, 1000 steps
+
+Material: ``E = 7e6*exp(0.2 z)``, ``h = 0.04*exp(0.1 z')`` with z, z' independent
+per-element GMRF samples (:mod:`cvfes_b200.gmrf`); nu = 0.49, rho = 1,
+mass-proportional damping 100 1/s; internal pressure ramped linearly to
+1.33e5 dyn/cm^2 over the first 100 steps; both end rings clamped.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import gmrf as _gmrf
+from .mesh import SolidMesh, TubeGeometry, stenosis_radius, tube_mesh, cfl_dt
+
+P_MAX = 1.33e5
+RAMP_STEPS = 100
+
+
+@dataclass
+class TubeCase:
+    name: str
+    nc: int
+    na: int
+    length: float
+    radius: float = 0.3
+    stenosed: bool = False
+    n_samples: int = 8
+    dt: Optional[float] = 2e-6
+    n_steps: int = 400
+    seed_E: int = 23
+    seed_h: int = 24
+    E0: float = 7.0e6
+    sigma_logE: float = 0.2
+    h0: float = 0.04
+    sigma_logh: float = 0.1
+    nu: float = 0.49
+    density: float = 1.0
+    damp: float = 100.0
+    tau: float = 0.1
+    marginal: str = "exact"
+    extra: dict = field(default_factory=dict)
+
+    def geometry(self) -> TubeGeometry:
+        rfn = (lambda x: stenosis_radius(x, r0=self.radius)) if self.stenosed else None
+        return TubeGeometry(self.nc, self.na, self.length, self.radius, rfn)
+
+    def pressures(self, n_steps: Optional[int] = None) -> np.ndarray:
+        n = self.n_steps if n_steps is None else n_steps
+        return P_MAX * np.minimum(np.arange(n, dtype=np.float64) / RAMP_STEPS, 1.0)
+
+
+CASES = {
+    "tube64x128": TubeCase("tube64x128", 64, 128, 3.0, n_samples=8, dt=2e-6, n_steps=400),
+    "tube256x1024": TubeCase("tube256x1024", 256, 1024, 3.0, n_samples=512, dt=5e-7, n_steps=2000),
+    "adjoint64": TubeCase("adjoint64", 64, 128, 3.0, n_samples=64, dt=2e-6, n_steps=500,
+                          extra=dict(n_obs=512, obs_every=10, ckpt_every=50)),
+    "stenosed512x2048": TubeCase("stenosed512x2048", 512, 2048, 5.0, stenosed=True,
+                                 n_samples=128, dt=None, n_steps=1000,
+                                 extra=dict(n_obs=4096, obs_every=10, ckpt_every=100)),
+}
+
+
+def _cache_dir() -> str:
+    d = os.environ.get("CVFES_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "cvfes_b200"))
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def build_mesh(case: TubeCase, n_samples: Optional[int] = None, cache: bool = True) -> SolidMesh:
+    """Generate the tube, its boundary rings and GMRF material (cached on disk)."""
+    S = case.n_samples if n_samples is None else n_samples
+    nodes, elems, inlet, outlet = tube_mesh(case.geometry())
+    key = hashlib.sha1(repr((case.nc, case.na, case.length, case.radius, case.stenosed, S,
+                             case.seed_E, case.seed_h, case.E0, case.sigma_logE, case.h0,
+                             case.sigma_logh, case.tau, case.marginal)).encode()).hexdigest()[:16]
+    path = os.path.join(_cache_dir(), f"{case.name}_{S}_{key}.npz")
+    if cache and os.path.exists(path):
+        d = np.load(path)
+        elmE, elmH = d["elmE"], d["elmThick"]
+    else:
+        elmE, elmH, _ = _gmrf.material_fields(elems, len(nodes), S, case.seed_E, case.seed_h,
+                                              case.E0, case.sigma_logE, case.h0, case.sigma_logh,
+                                              case.tau, case.marginal)
+        if cache:
+            np.savez(path, elmE=elmE, elmThick=elmH)
+    return SolidMesh(nodes=nodes, elementNodeIds=elems, boundary=np.concatenate([inlet, outlet]),
+                     nSmp=S, density=case.density, v=case.nu, damp=case.damp, bdyU=0.0,
+                     elmE=elmE, elmThick=elmH, name=case.name)
+
+
+def case_dt(case: TubeCase, mesh: SolidMesh) -> float:
+    """The case's dt, or the CFL rule 0.5*h_min/sqrt(E_max/rho) when it has none."""
+    if case.dt is not None:
+        return case.dt
+    return cfl_dt(mesh.nodes, mesh.elementNodeIds, float(np.max(mesh.elmE)), case.density)
+
+
+def batched_cases(n_tubes: int = 64, seed: int = 7):
+    """The 64-tube uneven ensemble: random radius, length, resolution and sample count."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_tubes):
+        nc = int(rng.choice([32, 64, 128, 256]))
+        na = int(rng.integers(64, 1025))
+        S = int(rng.choice([16, 32, 64, 128, 256]))
+        out.append(TubeCase(f"batch{i:02d}", nc, na, float(rng.uniform(1.0, 6.0)),
+                            radius=float(rng.uniform(0.15, 0.6)), n_samples=S, dt=None,
+                            n_steps=1000, seed_E=1000 + i, seed_h=2000 + i))
+    return out

@@ -1,0 +1,628 @@
+// Per-step kernels of the ensemble membrane solid time step.
+//
+// Layout: state u[3N][S] with samples innermost.  One thread owns one node and
+// VEC consecutive samples; it walks the node's incident elements in fan order,
+// gathers the two other nodes' displacements (16-byte vector loads across
+// samples), multiplies by the element's 3x9 stiffness rows (shared by all
+// samples) and the element's per-sample coefficient E*h, and accumulates the
+// node's row of K_s u_s in registers.  No scatter, no atomics, no colouring:
+// every row is owned by exactly one thread.  The explicit damped update
+// (physicsSolver.py:272-285, physicsSolverSDampGPUs.cl:416-446) and the
+// Dirichlet rows are fused into the same pass, so each step reads u_n, u_{n-1},
+// the inverse mass and the coefficients once and writes u_{n+1} once.
+//
+// The update is evaluated in increment form
+//     dv = u_n - u_{n-1};  v = dv - eta*dv + w*(p*fhat - K u_n);  u_{n+1} = u_n + v
+//     eta = dt*damp/(1 + dt*damp/2),  w = dt^2/((1 + dt*damp/2) m)
+// which is the reference's (dt^2 f + 2 m u - dt^2 K u + (dt/2 c - m) u_prev)/(m + dt/2 c)
+// with c = damp*m, rearranged so that the coefficients multiplying u_n carry no
+// rounding error (this matters for the FP32 state form).
+//
+// FP32 form (DIFF): each element row is applied to neighbour differences
+// (u_b - u_a); the self block is minus the sum of the two others, so rigid
+// translations are exactly in the null space and the FP32 cancellation error
+// scales with |u_b - u_a| instead of |u|.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace cvfes {
+
+template <typename T>
+struct StepArgs {
+    const int32_t* node_ptr;
+    const int4* rec;
+    const T* slab;
+    const T* fhat;
+    const T* coef;
+    const T* invm;
+    const T* u;
+    const T* up;
+    T* un;
+    const T* trac;
+    const double* p_sched;
+    const long long* clock;
+    long long j;
+    double pressure;
+    long long n_nodes;
+    int S;
+    int n_clamped;
+    T clamp;
+    T eta;
+    T w0;
+};
+
+// Row a of K_s u_s for VEC samples starting at column col.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row(const int32_t* __restrict__ node_ptr,
+                                       const int4* __restrict__ rec, const T* __restrict__ slab,
+                                       const T* __restrict__ coef, const T* __restrict__ u,
+                                       size_t S, size_t col, long long a, const Vec<T, V> (&ua)[3],
+                                       Vec<T, V> (&acc)[3]) {
+    const int k0 = __ldg(node_ptr + a), k1 = __ldg(node_ptr + a + 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    Vec<T, V> carry[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) carry[d] = vzero<T, V>();
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k) {
+        const int4 r = __ldg(rec + k);
+        Vec<T, V> x1[3], x2[3];
+        if (r.w & 1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x1[d] = carry[d];
+        } else {
+            const T* p1 = u + (size_t)r.y * 3 * S + col;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x1[d] = ldg<T, V>(p1 + d * S);
+                if constexpr (DIFF) x1[d] = vsub(x1[d], ua[d]);
+            }
+        }
+        const T* p2 = u + (size_t)r.z * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x2[d] = ldg<T, V>(p2 + d * S);
+            if constexpr (DIFF) x2[d] = vsub(x2[d], ua[d]);
+        }
+        const Vec<T, V> c = ldg<T, V>(coef + (size_t)r.x * S + col);
+        const T* K = slab + (size_t)kSlabStride * k;
+        T kk[27];
+        if constexpr (std::is_same<T, float>::value) {
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const float4 t = __ldg(reinterpret_cast<const float4*>(K) + q);
+                if (4 * q + 0 < 27) kk[4 * q + 0] = t.x;
+                if (4 * q + 1 < 27) kk[4 * q + 1] = t.y;
+                if (4 * q + 2 < 27) kk[4 * q + 2] = t.z;
+                if (4 * q + 3 < 27) kk[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 14; ++q) {
+                const double2 t = __ldg(reinterpret_cast<const double2*>(K) + q);
+                if (2 * q + 0 < 27) kk[2 * q + 0] = t.x;
+                if (2 * q + 1 < 27) kk[2 * q + 1] = t.y;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            Vec<T, V> t = vzero<T, V>();
+            if constexpr (!DIFF) {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], x1[jj]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], x2[jj]);
+            vfma(acc[i], c, t);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) carry[d] = x2[d];
+    }
+}
+
+template <typename T, int V, bool DIFF>
+__global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int SV = A.S / V;
+    const long long a = g / SV;
+    if (a >= A.n_nodes) return;
+    const size_t S = (size_t)A.S;
+    const size_t col = (size_t)(g - a * SV) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    if (a < A.n_clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    Vec<T, V> ua[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
+    Vec<T, V> acc[3];
+    ku_row<T, V, DIFF>(A.node_ptr, A.rec, A.slab, A.coef, A.u, S, col, a, ua, acc);
+
+    const double pd = A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure;
+    const T p = (T)pd;
+    const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
+    const T* fh = A.fhat + 4 * a;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const Vec<T, V> up = ldcs<T, V>(A.up + row + d * S);
+        T load = p * __ldg(fh + d);
+        if (A.trac) load += __ldg(A.trac + 4 * a + d);
+        Vec<T, V> o;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const T dv = ua[d].v[i] - up.v[i];
+            const T w = A.w0 * im.v[i];
+            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+        }
+        stcs<T, V>(A.un + row + d * S, o);
+    }
+}
+
+template <typename T, int V, bool DIFF>
+__global__ void __launch_bounds__(256)
+    k_kmul(const int32_t* node_ptr, const int4* rec, const T* slab, const T* coef, const T* u,
+           T* res, long long n_nodes, int S_, int accumulate) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int SV = S_ / V;
+    const long long a = g / SV;
+    if (a >= n_nodes) return;
+    const size_t S = (size_t)S_;
+    const size_t col = (size_t)(g - a * SV) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    Vec<T, V> ua[3], acc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(u + row + d * S);
+    ku_row<T, V, DIFF>(node_ptr, rec, slab, coef, u, S, col, a, ua, acc);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        Vec<T, V> o = acc[d];
+        if (accumulate) {
+            const Vec<T, V> r = ld<T, V>(res + row + d * S);
+#pragma unroll
+            for (int i = 0; i < V; ++i) o.v[i] += r.v[i];
+        }
+        st<T, V>(res + row + d * S, o);
+    }
+}
+
+// u_prev = u0 - dt du0 + dt^2/2 ddu0, ddu0 = (p0 f - damp m du0 - K u0)/m  (0 where m == 0).
+template <typename T>
+__global__ void k_init(const T* fhat, const T* invm, const T* u0, const T* du0, const T* ku,
+                       T* u_prev, long long n_nodes, int S, T p0, T dt, T damp) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long a = g / S;
+    if (a >= n_nodes) return;
+    const int s = (int)(g - a * S);
+    const T im = invm[(size_t)a * S + s];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const size_t o = ((size_t)a * 3 + d) * S + s;
+        const T m = im != T(0) ? T(1) / im : T(0);
+        const T rhs = p0 * fhat[4 * a + d] - damp * m * du0[o] - ku[o];
+        const T acc = im != T(0) ? rhs * im : T(0);
+        u_prev[o] = u0[o] - dt * du0[o] + T(0.5) * dt * dt * acc;
+    }
+}
+
+// res += K v in the reference layout K[nnzb][S][3][3] (MultiplyByVector).
+__global__ void k_bsr_spmv(long long n_nodes, int S, const long long* __restrict__ indptr,
+                           const long long* __restrict__ indices, const double* __restrict__ K,
+                           const double* __restrict__ v, double* __restrict__ res) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long a = g / S;
+    if (a >= n_nodes) return;
+    const int s = (int)(g - a * S);
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    for (long long ia = indptr[a]; ia < indptr[a + 1]; ++ia) {
+        const long long b = indices[ia];
+        const double* m = K + ((size_t)ia * S + s) * 9;
+        const double v0 = v[(3 * b) * S + s], v1 = v[(3 * b + 1) * S + s],
+                     v2 = v[(3 * b + 2) * S + s];
+        r0 += m[0] * v0 + m[1] * v1 + m[2] * v2;
+        r1 += m[3] * v0 + m[4] * v1 + m[5] * v2;
+        r2 += m[6] * v0 + m[7] * v1 + m[8] * v2;
+    }
+    res[(3 * a) * S + s] += r0;
+    res[(3 * a + 1) * S + s] += r1;
+    res[(3 * a + 2) * S + s] += r2;
+}
+
+__global__ void k_clock_add(long long* clock, long long n) { clock[0] += n; }
+
+// ------------------------------------------------------------------ norms
+constexpr int kNormThreads = 128;
+inline long long norm_chunks(long long n_nodes) {
+    long long c = (n_nodes + 63) / 64;
+    return std::max(1LL, std::min(1024LL, c));
+}
+
+template <typename T>
+__global__ void k_norms_partial(long long n_nodes, int S, long long npc, const T* __restrict__ u,
+                                const T* __restrict__ up, const T* __restrict__ invm,
+                                double* __restrict__ work) {
+    const long long chunk = blockIdx.x;
+    const int s = blockIdx.y * kNormThreads + threadIdx.x;
+    if (s >= S) return;
+    const long long a0 = chunk * npc, a1 = (a0 + npc < n_nodes) ? a0 + npc : n_nodes;
+    double su = 0.0, sv = 0.0, sm = 0.0, nf = 0.0;
+    for (long long a = a0; a < a1; ++a) {
+        const double im = (double)invm[(size_t)a * S + s];
+        const double m = im != 0.0 ? 1.0 / im : 0.0;
+        double dv2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const size_t o = ((size_t)a * 3 + d) * S + s;
+            const double x = (double)u[o], y = (double)up[o];
+            if (!isfinite(x)) nf += 1.0;
+            su += x * x;
+            dv2 += (x - y) * (x - y);
+        }
+        sv += dv2;
+        sm += m * dv2;
+    }
+    double* w = work + ((size_t)chunk * S + s) * 4;
+    w[0] = su;
+    w[1] = sv;
+    w[2] = sm;
+    w[3] = nf;
+}
+
+__global__ void k_norms_final(long long n_chunks, int S, const double* __restrict__ work,
+                              double* __restrict__ out, double* __restrict__ total_nonfinite) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * S) return;
+    const int s = t / 4, q = t % 4;
+    double acc = 0.0;
+    for (long long c = 0; c < n_chunks; ++c) acc += work[((size_t)c * S + s) * 4 + q];
+    out[(size_t)s * 4 + q] = acc;
+    if (q == 3 && acc != 0.0) atomicAdd(total_nonfinite, acc);
+}
+
+// ------------------------------------------------------------------ launchers
+template <typename T>
+int pick_vec(const void* const* ptrs, int n, int S) {
+    const int maxv = (int)(16 / sizeof(T));
+    for (int v = maxv; v > 1; v /= 2) {
+        if (S % v) continue;
+        bool ok = true;
+        for (int i = 0; i < n; ++i)
+            if (ptrs[i] && (reinterpret_cast<uintptr_t>(ptrs[i]) % (v * sizeof(T)))) ok = false;
+        if (ok) return v;
+    }
+    return 1;
+}
+
+int check_mesh(const cvfes_solid_mesh* m, const char* who) {
+    if (!m || m->n_nodes <= 0 || m->n_samples <= 0 || !m->node_ptr || !m->slot_rec ||
+        !m->slot_k || !m->fhat)
+        return fail(CVFES_ERR_ARG, "%s: incomplete mesh descriptor", who);
+    if (m->n_samples > INT32_MAX || m->n_clamped < 0 || m->n_clamped > m->n_nodes)
+        return fail(CVFES_ERR_ARG, "%s: bad sample count or clamped-row count", who);
+    if (reinterpret_cast<uintptr_t>(m->slot_k) % 16 || reinterpret_cast<uintptr_t>(m->slot_rec) % 16)
+        return fail(CVFES_ERR_ARG, "%s: slot arrays must be 16-byte aligned", who);
+    return CVFES_OK;
+}
+
+template <typename T>
+int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u,
+                const T* up, T* un, const double* p_sched, const long long* clock, long long j,
+                double pressure, const T* trac, double dt, double damp, cudaStream_t st) {
+    int rc = check_mesh(m, "cvfes_solid_step");
+    if (rc) return rc;
+    if (!coef || !invm || !u || !up || !un)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_step: null state pointer");
+    if (!(dt > 0.0)) return fail(CVFES_ERR_ARG, "cvfes_solid_step: dt must be positive");
+    StepArgs<T> A;
+    A.node_ptr = m->node_ptr;
+    A.rec = reinterpret_cast<const int4*>(m->slot_rec);
+    A.slab = static_cast<const T*>(m->slot_k);
+    A.fhat = static_cast<const T*>(m->fhat);
+    A.coef = coef;
+    A.invm = invm;
+    A.u = u;
+    A.up = up;
+    A.un = un;
+    A.trac = trac;
+    A.p_sched = p_sched;
+    A.clock = clock;
+    A.j = j;
+    A.pressure = pressure;
+    A.n_nodes = m->n_nodes;
+    A.S = (int)m->n_samples;
+    A.n_clamped = (int)m->n_clamped;
+    A.clamp = (T)m->clamp_value;
+    const double g = 0.5 * dt * damp;
+    A.eta = (T)(dt * damp / (1.0 + g));
+    A.w0 = (T)(dt * dt / (1.0 + g));
+    const void* ptrs[6] = {coef, invm, u, up, un, nullptr};
+    const int V = pick_vec<T>(ptrs, 5, A.S);
+    const int block = 256;
+    const unsigned grid = grid_1d(m->n_nodes * (A.S / V), block);
+    constexpr bool DIFF = std::is_same<T, float>::value;
+    if (V == 4) {
+        if constexpr (sizeof(T) == 4) k_step<T, 4, DIFF><<<grid, block, 0, st>>>(A);
+    } else if (V == 2) {
+        k_step<T, 2, DIFF><<<grid, block, 0, st>>>(A);
+    } else {
+        k_step<T, 1, DIFF><<<grid, block, 0, st>>>(A);
+    }
+    CVFES_LAUNCH_CHECK("k_step");
+    return CVFES_OK;
+}
+
+template <typename T>
+int launch_kmul(const cvfes_solid_mesh* m, const T* coef, const T* u, T* res, int accumulate,
+                cudaStream_t st) {
+    int rc = check_mesh(m, "cvfes_solid_kmul");
+    if (rc) return rc;
+    if (!coef || !u || !res) return fail(CVFES_ERR_ARG, "cvfes_solid_kmul: null pointer");
+    const int S = (int)m->n_samples;
+    const void* ptrs[3] = {coef, u, res};
+    const int V = pick_vec<T>(ptrs, 3, S);
+    const int block = 256;
+    const unsigned grid = grid_1d(m->n_nodes * (S / V), block);
+    constexpr bool DIFF = std::is_same<T, float>::value;
+    const int4* rec = reinterpret_cast<const int4*>(m->slot_rec);
+    const T* slab = static_cast<const T*>(m->slot_k);
+    if (V == 4) {
+        if constexpr (sizeof(T) == 4)
+            k_kmul<T, 4, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
+                                                       m->n_nodes, S, accumulate);
+    } else if (V == 2) {
+        k_kmul<T, 2, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
+                                                   m->n_nodes, S, accumulate);
+    } else {
+        k_kmul<T, 1, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
+                                                   m->n_nodes, S, accumulate);
+    }
+    CVFES_LAUNCH_CHECK("k_kmul");
+    return CVFES_OK;
+}
+
+template <typename T>
+int launch_advance(const cvfes_solid_mesh* m, const T* coef, const T* invm, T* b0, T* b1, T* b2,
+                   const double* p_sched, long long* clock, long long n_steps, double dt,
+                   double damp, int* cur_idx, int* prev_idx, cudaStream_t st) {
+    if (n_steps < 0) return fail(CVFES_ERR_ARG, "cvfes_solid_advance: negative step count");
+    if (!p_sched) return fail(CVFES_ERR_ARG, "cvfes_solid_advance: needs a pressure schedule");
+    T* buf[3] = {b0, b1, b2};
+    int cur = 0, prev = 1, nxt = 2;
+    for (long long j = 0; j < n_steps; ++j) {
+        int rc = launch_step<T>(m, coef, invm, buf[cur], buf[prev], buf[nxt], p_sched, clock, j,
+                                0.0, nullptr, dt, damp, st);
+        if (rc) return rc;
+        const int old_prev = prev;
+        prev = cur;
+        cur = nxt;
+        nxt = old_prev;
+    }
+    if (clock && n_steps > 0) {
+        k_clock_add<<<1, 1, 0, st>>>(clock, n_steps);
+        CVFES_LAUNCH_CHECK("k_clock_add");
+    }
+    if (cur_idx) *cur_idx = cur;
+    if (prev_idx) *prev_idx = prev;
+    return CVFES_OK;
+}
+
+template <typename T>
+int launch_init(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u0,
+                const T* du0, T* u_prev, T* work, double p0, double dt, double damp,
+                cudaStream_t st) {
+    if (!u0 || !du0 || !u_prev || !work || !invm)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_init: null pointer");
+    int rc = launch_kmul<T>(m, coef, u0, work, 0, st);
+    if (rc) return rc;
+    const int S = (int)m->n_samples;
+    const int block = 256;
+    k_init<T><<<grid_1d(m->n_nodes * S, block), block, 0, st>>>(
+        static_cast<const T*>(m->fhat), invm, u0, du0, work, u_prev, m->n_nodes, S, (T)p0, (T)dt,
+        (T)damp);
+    CVFES_LAUNCH_CHECK("k_init");
+    return CVFES_OK;
+}
+
+template <typename T>
+int launch_norms(long long n_nodes, long long S, const T* u, const T* up, const T* invm,
+                 double* work, double* out, int check_finite, cudaStream_t st) {
+    if (n_nodes <= 0 || S <= 0 || S > INT32_MAX || !u || !up || !invm || !work || !out)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_norms: bad argument");
+    const long long nch = norm_chunks(n_nodes);
+    const long long npc = (n_nodes + nch - 1) / nch;
+    double* total = work + (size_t)nch * S * 4;
+    CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
+    dim3 grid((unsigned)nch, (unsigned)((S + kNormThreads - 1) / kNormThreads));
+    k_norms_partial<T><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, up, invm, work);
+    CVFES_LAUNCH_CHECK("k_norms_partial");
+    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
+    CVFES_LAUNCH_CHECK("k_norms_final");
+    if (check_finite) {
+        double h = 0.0;
+        CVFES_CUDA_TRY(cudaMemcpyAsync(&h, total, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CVFES_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h != 0.0)
+            return fail(CVFES_ERR_NONFINITE, "watchdog: %.0f non-finite state values", h);
+    }
+    return CVFES_OK;
+}
+
+}  // namespace cvfes
+
+using namespace cvfes;
+
+extern "C" int cvfes_solid_kmul_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                    const double* u, double* res, int32_t accumulate,
+                                    void* stream) {
+    return launch_kmul<double>(mesh, coef, u, res, accumulate, (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_kmul_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                    const float* u, float* res, int32_t accumulate,
+                                    void* stream) {
+    return launch_kmul<float>(mesh, coef, u, res, accumulate, (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_solid_step_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                    const double* invm, const double* u, const double* u_prev,
+                                    double* u_next, const double* p_sched, const int64_t* clock,
+                                    int64_t j, double pressure, const double* trac, double dt,
+                                    double damp, void* stream) {
+    return launch_step<double>(mesh, coef, invm, u, u_prev, u_next, p_sched,
+                               reinterpret_cast<const long long*>(clock), j, pressure, trac, dt,
+                               damp, (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                    const float* invm, const float* u, const float* u_prev,
+                                    float* u_next, const double* p_sched, const int64_t* clock,
+                                    int64_t j, double pressure, const float* trac, double dt,
+                                    double damp, void* stream) {
+    return launch_step<float>(mesh, coef, invm, u, u_prev, u_next, p_sched,
+                              reinterpret_cast<const long long*>(clock), j, pressure, trac, dt,
+                              damp, (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_solid_advance_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                       const double* invm, double* buf0, double* buf1,
+                                       double* buf2, const double* p_sched, int64_t* clock,
+                                       int64_t n_steps, double dt, double damp, int32_t* cur_idx,
+                                       int32_t* prev_idx, void* stream) {
+    return launch_advance<double>(mesh, coef, invm, buf0, buf1, buf2, p_sched,
+                                  reinterpret_cast<long long*>(clock), n_steps, dt, damp,
+                                  cur_idx, prev_idx, (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_advance_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                       const float* invm, float* buf0, float* buf1, float* buf2,
+                                       const double* p_sched, int64_t* clock, int64_t n_steps,
+                                       double dt, double damp, int32_t* cur_idx,
+                                       int32_t* prev_idx, void* stream) {
+    return launch_advance<float>(mesh, coef, invm, buf0, buf1, buf2, p_sched,
+                                 reinterpret_cast<long long*>(clock), n_steps, dt, damp, cur_idx,
+                                 prev_idx, (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_solid_init_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                    const double* invm, const double* u0, const double* du0,
+                                    double* u_prev, double* work, double p0, double dt,
+                                    double damp, void* stream) {
+    return launch_init<double>(mesh, coef, invm, u0, du0, u_prev, work, p0, dt, damp,
+                               (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_init_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                    const float* invm, const float* u0, const float* du0,
+                                    float* u_prev, float* work, double p0, double dt, double damp,
+                                    void* stream) {
+    return launch_init<float>(mesh, coef, invm, u0, du0, u_prev, work, p0, dt, damp,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_bsr_spmv_f64(int64_t n_nodes, int64_t n_samples, const int64_t* indptr,
+                                  const int64_t* indices, const double* K, const double* v,
+                                  double* res, void* stream) {
+    if (n_nodes <= 0 || n_samples <= 0 || n_samples > INT32_MAX || !indptr || !indices || !K ||
+        !v || !res)
+        return fail(CVFES_ERR_ARG, "cvfes_bsr_spmv_f64: bad argument");
+    k_bsr_spmv<<<grid_1d(n_nodes * n_samples, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_nodes, (int)n_samples, reinterpret_cast<const long long*>(indptr),
+        reinterpret_cast<const long long*>(indices), K, v, res);
+    CVFES_LAUNCH_CHECK("k_bsr_spmv");
+    return CVFES_OK;
+}
+
+extern "C" int64_t cvfes_norms_work_size(int64_t n_nodes, int64_t n_samples) {
+    if (n_nodes <= 0 || n_samples <= 0) return 0;
+    return norm_chunks(n_nodes) * n_samples * 4 + 1;
+}
+
+extern "C" int cvfes_solid_norms_f64(int64_t n_nodes, int64_t n_samples, const double* u,
+                                     const double* u_prev, const double* invm, double* work,
+                                     double* out, int32_t check_finite, void* stream) {
+    return launch_norms<double>(n_nodes, n_samples, u, u_prev, invm, work, out, check_finite,
+                                (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_norms_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                                     const float* u_prev, const float* invm, double* work,
+                                     double* out, int32_t check_finite, void* stream) {
+    return launch_norms<float>(n_nodes, n_samples, u, u_prev, invm, work, out, check_finite,
+                               (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------ CUDA graphs
+struct cvfes_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int cvfes_graph_capture_advance(const cvfes_solid_mesh* mesh, int32_t precision,
+                                           const void* coef, const void* invm, void* buf0,
+                                           void* buf1, void* buf2, const double* p_sched,
+                                           int64_t* clock, int64_t chunk, double dt, double damp,
+                                           void* stream, cvfes_graph** out) {
+    (void)stream;
+    if (!out || chunk <= 0 || chunk % 3 != 0 || !clock)
+        return fail(CVFES_ERR_ARG,
+                    "cvfes_graph_capture_advance: chunk must be a positive multiple of 3 and a "
+                    "clock is required");
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_graph_capture_advance: precision must be 32 or 64");
+    cudaStream_t cs;
+    CVFES_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return fail(CVFES_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    }
+    int rc;
+    if (precision == 64)
+        rc = launch_advance<double>(mesh, (const double*)coef, (const double*)invm, (double*)buf0,
+                                    (double*)buf1, (double*)buf2, p_sched,
+                                    reinterpret_cast<long long*>(clock), chunk, dt, damp, nullptr,
+                                    nullptr, cs);
+    else
+        rc = launch_advance<float>(mesh, (const float*)coef, (const float*)invm, (float*)buf0,
+                                   (float*)buf1, (float*)buf2, p_sched,
+                                   reinterpret_cast<long long*>(clock), chunk, dt, damp, nullptr,
+                                   nullptr, cs);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CVFES_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(CVFES_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    }
+    cvfes_graph* g = new cvfes_graph;
+    g->graph = graph;
+    g->exec = exec;
+    *out = g;
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_graph_launch(cvfes_graph* g, void* stream) {
+    if (!g || !g->exec) return fail(CVFES_ERR_ARG, "cvfes_graph_launch: null graph");
+    CVFES_CUDA_TRY(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_graph_destroy(cvfes_graph* g) {
+    if (!g) return CVFES_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return CVFES_OK;
+}

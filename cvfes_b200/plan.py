@@ -1,0 +1,163 @@
+"""Device-resident set-up of one membrane mesh for the sm_100a solid step.
+
+A :class:`SolidPlan` owns (as torch CUDA tensors) everything the per-step
+kernels read that does not depend on the samples' state:
+
+* the node-centric slot layout (fan-ordered incident elements) built on the
+  host by ``cvfes_mesh_incidence``;
+* per-slot 3x9 rows of the unit element stiffness ``Kt_e`` (FP64, and an FP32
+  copy), built on the GPU by ``cvfes_solid_templates_f64``;
+* per-sample material: the stiffness coefficient ``E*h`` per element, the
+  lumped mass and its FP64 inverse per node, and the unit-pressure load.
+
+Tables (D, quadrature, lumped-mass weights) follow ``physicsSolver.py:146-197``.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+
+SHEAR_K = 5.0 / 6.0
+# Mid-edge quadrature of physicsSolver.py:146-148: (N_0, N_1, N_2, weight).
+QUAD = np.array([[0.5, 0.5, 0.0, 1.0 / 3.0],
+                 [0.5, 0.0, 0.5, 1.0 / 3.0],
+                 [0.0, 0.5, 0.5, 1.0 / 3.0]])
+SLAB = 28
+
+
+def d_matrix(v: float, k: float = SHEAR_K) -> np.ndarray:
+    """Membrane/transverse-shear constitutive matrix divided by E (physicsSolver.py:184-188)."""
+    c = 1.0 - v * v
+    D = np.zeros((5, 5))
+    D[0, 0] = D[1, 1] = 1.0 / c
+    D[0, 1] = D[1, 0] = v / c
+    D[2, 2] = 0.5 * (1 - v) / c
+    D[3, 3] = D[4, 4] = 0.5 * k * (1 - v) / c
+    return D
+
+
+def lumped_mass_weights(density: float) -> np.ndarray:
+    """mw[a, g] = rho * w_g^2 * N_g(a): row sum of tM_g * w_g for local node a
+    (tM_g = N_gᵀN_g w_g rho, physicsSolver.py:190-197; the assembly multiplies
+    by w_g once more, optimizedSolidAssemble.pyx:564-566)."""
+    return density * (QUAD[:, :3] * (QUAD[:, 3:4] ** 2)).T.copy()
+
+
+def incidence(elements: np.ndarray, n_nodes: int):
+    """Host call of ``cvfes_mesh_incidence``: (node_ptr, slot_rec (3E,4), elem_slot (E,3))."""
+    e = np.ascontiguousarray(elements, dtype=np.int64)
+    E = e.shape[0]
+    node_ptr = np.empty(n_nodes + 1, dtype=np.int32)
+    slot_rec = np.empty((3 * E, 4), dtype=np.int32)
+    elem_slot = np.empty((E, 3), dtype=np.int32)
+    call("cvfes_mesh_incidence", n_nodes, E, ptr(e), ptr(node_ptr), ptr(slot_rec), ptr(elem_slot))
+    return node_ptr, slot_rec, elem_slot
+
+
+def color_greedy(elements: np.ndarray, n_nodes: int, max_colors: int = 23):
+    """Host call of ``cvfes_mesh_color_greedy`` (meshColoring.py semantics)."""
+    e = np.ascontiguousarray(elements, dtype=np.int64)
+    colors = np.empty(e.shape[0], dtype=np.int32)
+    n = call("cvfes_mesh_color_greedy", n_nodes, e.shape[0], ptr(e), max_colors, ptr(colors))
+    return colors, n
+
+
+class SolidPlan:
+    """Mesh-dependent device data of the solid step (one mesh, local numbering).
+
+    ``nodes (N,3)`` and ``elements (E,3)`` must already be in the solver's local
+    numbering with the clamped nodes first (``n_clamped`` of them).
+    """
+
+    def __init__(self, nodes, elements, n_clamped: int, clamp_value: float, v: float,
+                 density: float, device="cuda", precisions=(32, 64), keep_full=False):
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise RuntimeError("SolidPlan needs a CUDA device; there is no CPU path")
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        elements = np.ascontiguousarray(elements, dtype=np.int64)
+        self.N = int(nodes.shape[0])
+        self.E = int(elements.shape[0])
+        self.n_clamped = int(n_clamped)
+        self.clamp_value = float(clamp_value)
+        self.v = float(v)
+        self.density = float(density)
+        self.precisions = tuple(precisions)
+        node_ptr, slot_rec, elem_slot = incidence(elements, self.N)
+        self.host_node_ptr, self.host_slot_rec = node_ptr, slot_rec
+        dev = self.device
+        self.stream = torch.cuda.current_stream(dev)
+        self.nodes = torch.from_numpy(nodes).to(dev)
+        self.elems = torch.from_numpy(elements.astype(np.int32)).to(dev)
+        self.node_ptr = torch.from_numpy(node_ptr).to(dev)
+        self.slot_rec = torch.from_numpy(slot_rec).to(dev)
+        self.elem_slot = torch.from_numpy(elem_slot).to(dev)
+        ns = 3 * self.E
+        self.slot_k64 = torch.empty(SLAB * ns, dtype=torch.float64, device=dev) if 64 in self.precisions else None
+        self.slot_k32 = torch.empty(SLAB * ns, dtype=torch.float32, device=dev) if 32 in self.precisions else None
+        self.kt_full = torch.empty(self.E * 81, dtype=torch.float64, device=dev) if keep_full else None
+        self.area = torch.empty(self.E, dtype=torch.float64, device=dev)
+        self.normal = torch.empty(3 * self.E, dtype=torch.float64, device=dev)
+        D = np.ascontiguousarray(d_matrix(self.v))
+        with torch.cuda.device(dev):
+            call("cvfes_solid_templates_f64", self.N, self.E, ptr(self.nodes), ptr(self.elems),
+                 ptr(D), ptr(self.elem_slot), ptr(self.slot_rec), ptr(self.slot_k64),
+                 ptr(self.slot_k32), ptr(self.kt_full), ptr(self.area), ptr(self.normal),
+                 self._s())
+        self.S = None
+
+    def _s(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    # ------------------------------------------------------------------ material
+    def set_material(self, coefK, gthick):
+        """Per-sample material: ``coefK (E,S)`` = E*h weighted at the quadrature points and
+        thickness ``gthick`` as ``(E,S)`` (uniform per element) or ``(E,S,3)``."""
+        dev = self.device
+        coef64 = torch.as_tensor(np.ascontiguousarray(coefK, dtype=np.float64)).to(dev)
+        g = np.ascontiguousarray(gthick, dtype=np.float64)
+        if g.ndim == 3 and np.all(g == g[:, :, :1]):
+            g = np.ascontiguousarray(g[:, :, 0])
+        n_gauss = 1 if g.ndim == 2 else 3
+        if coef64.shape[0] != self.E or g.shape[0] != self.E or g.shape[1] != coef64.shape[1]:
+            raise ValueError("coefK/gthick must be (E,S) / (E,S[,3]) for this mesh")
+        S = int(coef64.shape[1])
+        self.S = S
+        gth = torch.from_numpy(g).to(dev)
+        self.coef64 = coef64 if 64 in self.precisions else None
+        self.coef32 = coef64.to(torch.float32) if 32 in self.precisions else None
+        self.lm = torch.empty((self.N, S), dtype=torch.float64, device=dev)
+        self.invm64 = torch.empty((self.N, S), dtype=torch.float64, device=dev)
+        self.invm32 = torch.empty((self.N, S), dtype=torch.float32, device=dev)
+        self.fhat64 = torch.empty((self.N, 4), dtype=torch.float64, device=dev)
+        self.fhat32 = torch.empty((self.N, 4), dtype=torch.float32, device=dev)
+        mw = np.ascontiguousarray(lumped_mass_weights(self.density))
+        with torch.cuda.device(dev):
+            call("cvfes_solid_mass_load_f64", self.N, self.E, S, ptr(self.node_ptr),
+                 ptr(self.slot_rec), ptr(self.area), ptr(self.normal), ptr(gth), n_gauss,
+                 ptr(mw), ptr(self.lm), ptr(self.invm64), ptr(self.invm32), ptr(self.fhat64),
+                 ptr(self.fhat32), self._s())
+        del gth
+        if 64 not in self.precisions:
+            self.invm64 = None
+        return self
+
+    def coef(self, precision):
+        return self.coef64 if precision == 64 else self.coef32
+
+    def invm(self, precision):
+        return self.invm64 if precision == 64 else self.invm32
+
+    def desc(self, precision: int) -> _lib.SolidMeshDesc:
+        """C descriptor of this mesh for FP32 or FP64 kernels (valid while self lives)."""
+        if self.S is None:
+            raise RuntimeError("set_material() first")
+        slab = self.slot_k64 if precision == 64 else self.slot_k32
+        fhat = self.fhat64 if precision == 64 else self.fhat32
+        if slab is None:
+            raise RuntimeError(f"plan was built without FP{precision} templates")
+        return _lib.SolidMeshDesc(self.N, self.E, self.S, self.n_clamped, self.clamp_value,
+                                  ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat))

@@ -1,0 +1,374 @@
+"""Drop-in GPU solid solver with the reference's class interface.
+
+``GPUSolidSolver(comm, mesh, config)`` keeps the constructor and methods of the
+reference class (``physicsSolverSDampGPUs.py:45-496``; identical API in
+``physicsSolverGPUs.py:45-490``): ``RefreshContext(physicSolver)``,
+``Solve(t, dt)``, ``Save(filename, counter)``, ``ApplyBoundaryCondition``,
+``SyncCommNodes`` and ``UnionDisplacement``.  It is constructed the same way by
+``TransientSolverGPU`` (``solver.py:148-158``).
+
+Differences by design:
+* device memory is owned by torch tensors; every kernel is a libcvfes_b200
+  entry point (no OpenCL, no CPU fallback: without a CUDA device the
+  constructor raises);
+* the Dirichlet rows, the damping and the optional nodal traction are applied
+  on the device inside the step kernel, so a step makes no host round trip
+  (the reference copies the boundary rows to the host and back every step,
+  ``physicsSolverSDampGPUs.py:363-390``);
+* the stiffness is the linear template form: ``K_s = sum_e (E h)_{e,s} Kt_e``
+  assembled once on the undeformed wall (stiffness update interval infinite);
+* FP64 (default) or FP32 state, chosen by ``[gpu] precision``.
+"""
+from __future__ import annotations
+
+import math
+import os
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .plan import SolidPlan
+
+
+class LocalComm:
+    """Single-rank stand-in for an MPI communicator (mpi4py is not a dependency)."""
+
+    def Get_size(self):
+        return 1
+
+    def Get_rank(self):
+        return 0
+
+    def Barrier(self):
+        return None
+
+
+class PhysicsSolver:
+    """Protocol base of the physics step (``physicsSolver.py:53-84``)."""
+
+    Dof = 3
+
+    def __init__(self, comm, mesh, config):
+        self.comm = comm
+        self.size = comm.Get_size()
+        self.rank = comm.Get_rank()
+        self.mesh = mesh
+        self.Dof = mesh.dof if mesh is not None else 3
+        self.dt = config.dt
+
+    def RefreshContext(self, physicSolver):
+        pass
+
+    def Solve(self, t, dt):
+        pass
+
+    def Save(self, filename, counter):
+        pass
+
+    def Steady(self):
+        return False
+
+
+class FluidSolver(PhysicsSolver):
+    """Time source for the solid (``physicsSolver.py:87-99``): records ``t``."""
+
+    def __init__(self, comm, mesh, config):
+        PhysicsSolver.__init__(self, comm, mesh, config)
+        self.t = 0.0
+
+    def Solve(self, t, dt):
+        self.t = t
+
+
+def pressure_at(t: float, P: float, T: float, ramp: str) -> float:
+    """Load schedule of ``RefreshContext`` (physicsSolverSDampGPUs.py:317-322) or a linear ramp."""
+    if t > T:
+        return P
+    if ramp == "linear":
+        return P * t / T
+    return P / 2.0 - P / 2.0 * math.cos(math.pi / T * t)
+
+
+class GPUSolidSolver(PhysicsSolver):
+    """Ensemble membrane solid on one B200 (see module docstring)."""
+
+    def __init__(self, comm, mesh, config):
+        PhysicsSolver.__init__(self, comm, mesh, config)
+        gpu = getattr(config, "gpu", None)
+        self.precision = getattr(gpu, "precision", 64)
+        self.use_graph = getattr(gpu, "use_graph", True)
+        self.graph_chunk = getattr(gpu, "graph_chunk", 48)
+        self.watchdog = getattr(gpu, "watchdog", True)
+        self.InitializeSync()
+        if self.InitializeGPU(getattr(gpu, "device", -1)) < 0:
+            raise RuntimeError("GPUSolidSolver: no usable CUDA device")
+
+        self.dt_f = getattr(config, "dt_f", 0.01)
+        self.stressFilename = getattr(config, "exportBdyStressFilename", None)
+        self.useConstantStress = getattr(config, "useConstantStress", False)
+        self.constant_T = getattr(config, "constant_T", 1.0)
+        self.constantPressure = getattr(config, "constant_pressure", 0.0)
+        self.pressure_ramp = getattr(config, "pressure_ramp", "cosine")
+        self.nt = 0
+        if self.stressFilename is not None:
+            if self.useConstantStress:
+                self.etrac = np.load("{}.npy".format(self.stressFilename))
+            else:
+                self.strac = np.load("{}{}.npy".format(self.stressFilename, self.nt))
+                self.etrac = np.load("{}{}.npy".format(self.stressFilename, self.nt + 1))
+        else:
+            self.etrac = None
+        self.pressure = 0.0
+
+        self.nSmp = config.nSmp
+        self.ndof = mesh.ndof
+        self.nNodes = mesh.nNodes
+        self.nElms = mesh.nElements
+        self.lclNNodes = mesh.lclNNodes
+        self.lclNodeIds = mesh.lclNodeIds
+        self.lclElmNodeIds = mesh.lclElmNodeIds
+        self.lclNDof = self.lclNNodes * mesh.dof
+        self.lclNCommNodes = mesh.lclNCommNodes
+        self.lclNCommDof = self.lclNCommNodes * mesh.dof
+        self.lclNSpecialHeadDof = mesh.lclNSpecialHead * mesh.dof
+        self.lclBoundary = mesh.lclBoundary
+        self.damp = mesh.damp
+        self.dofs = (3 * self.lclNodeIds[:, None] + np.arange(3)[None, :]).ravel()
+        self.du = np.asarray(mesh.iniDu)[self.dofs]
+        self.u = np.asarray(mesh.iniU)[self.dofs]
+        self.InitializeSolver()
+
+    # ------------------------------------------------------------------ set-up
+    def InitializeGPU(self, device: int = -1) -> int:
+        """Pick the CUDA device of this rank (``physicsSolverSDampGPUs.py:107-131``)."""
+        if not torch.cuda.is_available():
+            return -1
+        n = torch.cuda.device_count()
+        if n < self.size:
+            print("GPUs is not enough! Actual size: {}, need: {}".format(n, self.size))
+            return -1
+        idx = device if device >= 0 else int(os.environ.get("LOCAL_RANK", self.rank)) % n
+        self.device = torch.device("cuda", idx)
+        _lib.load()
+        return 0
+
+    def InitializeSync(self):
+        self.bdyDofs = (3 * np.asarray(self.mesh.lclBoundary)[:, None] + np.arange(3)).ravel()
+        if self.size > 1:
+            raise NotImplementedError("GPUSolidSolver runs one mesh on one GPU; mesh partitioning "
+                                      "over ranks is outside this package")
+
+    def InitializeSolver(self):
+        """Templates, lumped mass, load and the Taylor start ``u_{-1}``
+        (``physicsSolverSDampGPUs.py:143-277``, ``physicsSolver.py:209-230``)."""
+        m = self.mesh
+        dev = self.device
+        with torch.cuda.device(dev):
+            self.plan = SolidPlan(m.nodes[self.lclNodeIds], self.lclElmNodeIds,
+                                  n_clamped=m.lclNSpecialHead, clamp_value=m.bdyU, v=m.v,
+                                  density=m.density, device=dev, precisions=(self.precision,))
+            coefK, gthick = m.element_coefficients()
+            self.plan.set_material(coefK, gthick)
+            self._desc = self.plan.desc(self.precision)
+            dtype = torch.float64 if self.precision == 64 else torch.float32
+            S, ndof = self.nSmp, self.lclNDof
+            self.bufs = [torch.zeros((ndof, S), dtype=dtype, device=dev) for _ in range(3)]
+            self.cur, self.prev, self.nxt = 0, 1, 2
+            u0 = torch.from_numpy(np.repeat(self.u[:, None], S, axis=1)).to(dev, dtype)
+            du0 = torch.from_numpy(np.repeat(self.du[:, None], S, axis=1)).to(dev, dtype)
+            self.bufs[self.cur].copy_(u0)
+            work = torch.empty_like(u0)
+            fn = "cvfes_solid_init_f64" if self.precision == 64 else "cvfes_solid_init_f32"
+            call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
+                 ptr(self.plan.invm(self.precision)), ptr(u0), ptr(du0),
+                 ptr(self.bufs[self.prev]), ptr(work), float(self.pressure), float(self.dt),
+                 float(self.damp), self._stream())
+            del work, u0, du0
+            self.trac_dev = None
+            self.clock = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.norm_work = torch.empty(
+                int(_lib.load().cvfes_norms_work_size(self.lclNNodes, S)), dtype=torch.float64,
+                device=dev)
+            self._graphs = {}
+            self._p_buf = None
+            self.step_count = 0
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    # ------------------------------------------------------------------ per step
+    def RefreshContext(self, physicSolver):
+        """Load at time ``physicSolver.t`` (``physicsSolverSDampGPUs.py:280-322``)."""
+        t = physicSolver.t
+        ramp_T = self.constant_T
+        if self.stressFilename is not None:
+            if self.useConstantStress:
+                if t > ramp_T:
+                    appTrac = self.etrac
+                else:
+                    appTrac = self.etrac / 2.0 - self.etrac / 2.0 * math.cos(math.pi / ramp_T * t)
+            else:
+                if t > ramp_T:
+                    if int((t - ramp_T) / self.dt_f) > self.nt:
+                        self.nt += 1
+                        self.strac = self.etrac
+                        self.etrac = np.load("{}{}.npy".format(self.stressFilename, self.nt + 1))
+                    appTrac = self.strac + (t - ramp_T - self.nt * self.dt_f) * \
+                        (self.etrac - self.strac) / self.dt_f
+                else:
+                    appTrac = self.strac / 2.0 - self.strac / 2.0 * math.cos(math.pi / ramp_T * t)
+            self.set_traction(appTrac)
+        self.pressure = pressure_at(t, self.constantPressure, self.constant_T, self.pressure_ramp)
+
+    def set_traction(self, appTrac):
+        """Nodal traction (N,3) in global node order; boundary rows are zeroed."""
+        tr = np.zeros((self.lclNNodes, 4))
+        tr[:, :3] = np.asarray(appTrac, dtype=np.float64).reshape(-1, 3)[self.lclNodeIds]
+        tr[self.lclBoundary, :] = 0.0
+        dtype = torch.float64 if self.precision == 64 else torch.float32
+        self.trac_dev = torch.from_numpy(tr).to(self.device, dtype)
+
+    def Solve(self, t, dt):
+        """One explicit step for all samples (``physicsSolverSDampGPUs.py:325-399``)."""
+        fn = "cvfes_solid_step_f64" if self.precision == 64 else "cvfes_solid_step_f32"
+        with torch.cuda.device(self.device):
+            call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
+                 ptr(self.plan.invm(self.precision)), ptr(self.bufs[self.cur]),
+                 ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), None, None, 0,
+                 float(self.pressure), ptr(self.trac_dev), float(dt), float(self.damp),
+                 self._stream())
+        self.prev, self.cur, self.nxt = self.cur, self.nxt, self.prev
+        self.step_count += 1
+
+    def Advance(self, pressures, dt: Optional[float] = None, use_graph: Optional[bool] = None):
+        """Many steps with a per-step pressure schedule, no host work between steps.
+
+        With ``use_graph`` the steps run as replays of one captured CUDA graph of
+        ``graph_chunk`` steps (a multiple of 3); the remainder runs as plain launches.
+        """
+        dt = self.dt if dt is None else dt
+        use_graph = self.use_graph if use_graph is None else use_graph
+        p = self._schedule(pressures)
+        n = int(p.numel())
+        prec = self.precision
+        with torch.cuda.device(self.device):
+            self.clock.zero_()
+            done = 0
+            chunk = self.graph_chunk
+            if use_graph and self.trac_dev is None and n >= chunk:
+                key = (chunk, float(dt), self.cur, self.prev, self.nxt, p.data_ptr())
+                g = self._graphs.get(key)
+                if g is None:
+                    for old in self._graphs.values():
+                        call("cvfes_graph_destroy", old)
+                    self._graphs.clear()
+                    h = _lib.C.c_void_p()
+                    b = self.bufs
+                    call("cvfes_graph_capture_advance", C_desc(self._desc), prec,
+                         ptr(self.plan.coef(prec)), ptr(self.plan.invm(prec)),
+                         ptr(b[self.cur]), ptr(b[self.prev]), ptr(b[self.nxt]), ptr(p),
+                         ptr(self.clock), chunk, float(dt), float(self.damp), self._stream(),
+                         _lib.C.byref(h))
+                    g = h.value
+                    self._graphs[key] = (g,)
+                else:
+                    g = g[0]
+                while n - done >= chunk:
+                    call("cvfes_graph_launch", g, self._stream())
+                    done += chunk
+            if n - done > 0:
+                cur_idx = _lib.C.c_int32()
+                prev_idx = _lib.C.c_int32()
+                if self.trac_dev is not None:
+                    for j in range(done, n):
+                        self.pressure = float(pressures[j])
+                        self.Solve(None, dt)
+                else:
+                    fn = "cvfes_solid_advance_f64" if prec == 64 else "cvfes_solid_advance_f32"
+                    b = self.bufs
+                    order = [self.cur, self.prev, self.nxt]
+                    call(fn, C_desc(self._desc), ptr(self.plan.coef(prec)),
+                         ptr(self.plan.invm(prec)), ptr(b[order[0]]), ptr(b[order[1]]),
+                         ptr(b[order[2]]), ptr(p), ptr(self.clock), n - done, float(dt),
+                         float(self.damp), _lib.C.byref(cur_idx), _lib.C.byref(prev_idx),
+                         self._stream())
+                    self.cur, self.prev = order[cur_idx.value], order[prev_idx.value]
+                    self.nxt = 3 - self.cur - self.prev
+            self.step_count += n
+        return self
+
+    def _schedule(self, pressures) -> torch.Tensor:
+        """Pressure schedule copied into a persistent device buffer: its address never
+        changes, so a captured graph (which reads ``p[clock + j]``) stays valid."""
+        if isinstance(pressures, torch.Tensor):
+            src = pressures.to(self.device, torch.float64).reshape(-1)
+        else:
+            src = torch.from_numpy(np.ascontiguousarray(pressures, dtype=np.float64).ravel())
+        n = int(src.numel())
+        if self._p_buf is None or self._p_buf.numel() < n:
+            self.release_graphs()
+            self._p_buf = torch.empty(max(n, 4096), dtype=torch.float64, device=self.device)
+        view = self._p_buf[:n]
+        view.copy_(src, non_blocking=True)
+        return view
+
+    def release_graphs(self):
+        for g in self._graphs.values():
+            call("cvfes_graph_destroy", g[0])
+        self._graphs.clear()
+
+    def __del__(self):
+        try:
+            self.release_graphs()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ outputs
+    def Norms(self, check_finite: Optional[bool] = None) -> np.ndarray:
+        """FP64 per-sample (sum u^2, sum du^2, sum m du^2, #non-finite), shape (S, 4)."""
+        out = torch.empty((self.nSmp, 4), dtype=torch.float64, device=self.device)
+        fn = "cvfes_solid_norms_f64" if self.precision == 64 else "cvfes_solid_norms_f32"
+        chk = self.watchdog if check_finite is None else check_finite
+        with torch.cuda.device(self.device):
+            call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
+                 ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
+                 ptr(self.norm_work), ptr(out), int(bool(chk)), self._stream())
+        return out.cpu().numpy()
+
+    def local_displacement(self) -> torch.Tensor:
+        """Current displacement (lclNDof, S) on the device, local node order."""
+        return self.bufs[self.cur]
+
+    def displacement(self) -> np.ndarray:
+        """Current displacement (ndof, S) as FP64 numpy in global node order."""
+        return self.UnionDisplacement(self.bufs[self.cur].double().cpu().numpy())
+
+    def ApplyBoundaryCondition(self, quant):
+        """Host-side Dirichlet rows (``physicsSolver.py:327-328``); the step kernel
+        applies the same rows on the device."""
+        quant[self.bdyDofs, :] = self.mesh.bdyU
+
+    def SyncCommNodes(self, quant):
+        """Shared-node sum over ranks; a single GPU owns every node, so nothing to do."""
+        return None
+
+    def UnionDisplacement(self, quant):
+        resU = np.empty((self.ndof, self.nSmp))
+        resU[self.dofs, :] = quant
+        return resU
+
+    def Save(self, filename, counter):
+        """Displacement of every sample at this step (``physicsSolverSDampGPUs.py:452-464``)."""
+        resU = self.displacement()
+        if self.rank == 0:
+            from .io import save_displacement
+            save_displacement(filename, counter, self.mesh,
+                              resU.T.reshape(self.nSmp, self.mesh.nNodes, self.Dof))
+        self.comm.Barrier()
+
+
+def C_desc(desc):
+    return _lib.C.byref(desc)

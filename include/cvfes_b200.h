@@ -1,0 +1,227 @@
+/*
+ * cvfes_b200 — C ABI of the B200 ensemble membrane solid time step.
+ *
+ * Plain pointers, sizes and a cudaStream_t passed as void*.  Every pointer
+ * documented as "device" must be device memory owned by the caller (the
+ * Python host layer passes torch tensors); the library never allocates state.
+ * Every function returns a status code (CVFES_OK == 0, negative on error) and
+ * records a message readable through cvfes_last_error().
+ *
+ * Layout conventions (identical to the reference's GPU buffers, which are
+ * (lclNDof, nSmp) C-order, sample innermost — physicsSolverSDampGPUs.py:188-269):
+ *   state / load vectors   T[3*N][S]   (dof-major, sample innermost)
+ *   per-element fields     T[E][S]
+ *   per-node fields        T[N][S]
+ *   Dirichlet rows         local nodes [0, n_clamped)   (boundary-first
+ *                          numbering, meshPartition.py:240-254)
+ *
+ * Each entry point cites the reference interface it replaces.
+ */
+#ifndef CVFES_B200_H
+#define CVFES_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CVFES_OK               0
+#define CVFES_ERR_ARG         -1   /* invalid argument (size, null, layout)       */
+#define CVFES_ERR_CUDA        -2   /* CUDA runtime error                          */
+#define CVFES_ERR_NONFINITE   -3   /* watchdog saw NaN/Inf in the state           */
+#define CVFES_ERR_TIMEOUT     -4   /* a bounded device wait gave up               */
+#define CVFES_ERR_UNSUPPORTED -5   /* configuration not supported by this build   */
+#define CVFES_ERR_MESH        -6   /* mesh preprocessing failed (e.g. colours)    */
+
+/* Node-centric view of a membrane mesh, all arrays device-resident.
+ * Slot k in [node_ptr[a], node_ptr[a+1]) is one element incident to node a.
+ *   slot_rec[4k+0] element id e
+ *   slot_rec[4k+1] first other node of e  (column block 1 of the slot rows)
+ *   slot_rec[4k+2] second other node of e (column block 2)
+ *   slot_rec[4k+3] bit0: block 1 equals block 2 of slot k-1 (fan order)
+ *                  bits 8..9: local index of a inside e
+ *   slot_k   [28k + 9q + 3i + j] = Kt_e[3*la+i][3*lb_q+j], q = 0 (a), 1, 2
+ *                                  (unit-coefficient element stiffness rows)
+ *   fhat     [4a + d]            unit-pressure nodal load, d < 3 (pad at 3)
+ */
+typedef struct cvfes_solid_mesh {
+    int64_t        n_nodes;
+    int64_t        n_elems;
+    int64_t        n_samples;
+    int64_t        n_clamped;
+    double         clamp_value;   /* bdyU of ApplyBoundaryCondition */
+    const int32_t* node_ptr;      /* [n_nodes + 1]    */
+    const int32_t* slot_rec;      /* [4 * n_slots]    */
+    const void*    slot_k;        /* [28 * n_slots] T */
+    const void*    fhat;          /* [4 * n_nodes]  T */
+} cvfes_solid_mesh;
+
+/* ---------------------------------------------------------------- errors */
+const char* cvfes_last_error(void);
+int         cvfes_version(void);
+
+/* ------------------------------------------------- host preprocessing (CPU)
+ * Node -> incident-element slots in fan order.  Replaces the node/element
+ * neighbour search of meshColoring.py:25-36 and gives the kernels their
+ * gather order.  elems is host int64 [E][3]; outputs host int32.
+ * node_ptr [N+1]; slot_rec [4*3E]; elem_slot [3E] (slot of (e, local node)). */
+int cvfes_mesh_incidence(int64_t n_nodes, int64_t n_elems, const int64_t* elems,
+                         int32_t* node_ptr, int32_t* slot_rec, int32_t* elem_slot);
+
+/* Greedy element colouring over the node-sharing graph, smallest free colour
+ * in element order (meshColoring.py:7-63).  colors: host int32 [E].
+ * Returns the number of colours (>0) or CVFES_ERR_MESH if max_colors is too few. */
+int cvfes_mesh_color_greedy(int64_t n_nodes, int64_t n_elems, const int64_t* elems,
+                            int32_t max_colors, int32_t* colors);
+
+/* Diagonal of Q^{-1} from a sparse factor Q = L D Lᵀ (selected inversion), for
+ * the exact unit-marginal rescaling of the GMRF material samples (the reference
+ * rescales by the empirical std across samples, GMRF.py:326-328).  L: host CSC,
+ * unit lower triangular, sorted rows (int64 colptr [n+1], rowind, f64 values);
+ * d host f64 [n]; out_diag host f64 [n].                                       */
+int cvfes_gmrf_selected_inverse_diag(int64_t n, const int64_t* colptr, const int64_t* rowind,
+                                     const double* lval, const double* d, double* out_diag);
+
+/* Solve Lᵀ X = B in place (L unit lower triangular, host CSC as above; B host
+ * f64 [n][nrhs], samples innermost): the X = L⁻ᵀ Z draw of GMRF.py:310, for
+ * many samples at once, OpenMP over sample columns.                           */
+int cvfes_gmrf_solve_lt(int64_t n, const int64_t* colptr, const int64_t* rowind,
+                        const double* lval, int64_t nrhs, double* b);
+
+/* --------------------------------------------------- one-time device set-up
+ * Element frames and unit stiffness templates in FP64 (replaces the per-element
+ * part of OptimizedSolidAssembleWithDamping, optimizedSolidAssemble.pyx:520-583,
+ * and the initial pass of assemble_K_M_P, physicsSolverSDampGPUs.cl:28-223).
+ *   nodes      device f64 [N][3]     elems device int32 [E][3]
+ *   dmat       host   f64 [5][5]     (D of physicsSolver.py:184-188, no E)
+ *   elem_slot  device int32 [3E]     slot_rec device int32 [4*3E]
+ * Outputs (device, any may be NULL): slot_k64 f64 [28*3E], slot_k32 f32 [28*3E],
+ *   kt_full f64 [E][81] (full 9x9), area f64 [E], normal f64 [E][3].        */
+int cvfes_solid_templates_f64(int64_t n_nodes, int64_t n_elems, const double* nodes,
+                              const int32_t* elems, const double* dmat,
+                              const int32_t* elem_slot, const int32_t* slot_rec,
+                              double* slot_k64, float* slot_k32, double* kt_full,
+                              double* area, double* normal, void* stream);
+
+/* Lumped mass and unit pressure load, FP64 (replaces lumpingWithDamping,
+ * optimizedSolidAssemble.pyx:434-454, and the traction part, pyx:585-590).
+ *   gthick  device f64 [E][S][n_gauss] thickness at the quadrature points;
+ *           n_gauss = 3 (one per mid-edge point) or 1 (same thickness at all 3)
+ *   mw      host f64 [3][3] row-sum weights mw[a][g] = rho * w_g^2 * N_g(a)
+ * Outputs: lm f64 [N][S] (lumped mass, same for x/y/z), invm64 f64 [N][S],
+ *   invm32 f32 [N][S] (1/lm, 0 where lm == 0), fhat64 f64 [N][4], fhat32 f32 [N][4]. */
+int cvfes_solid_mass_load_f64(int64_t n_nodes, int64_t n_elems, int64_t n_samples,
+                              const int32_t* node_ptr, const int32_t* slot_rec,
+                              const double* area, const double* normal,
+                              const double* gthick, int32_t n_gauss, const double* mw,
+                              double* lm, double* invm64, float* invm32,
+                              double* fhat64, float* fhat32, void* stream);
+
+/* Block-CSR assembly of K_s = sum_e coef[e,s] Kt_e into the reference layout
+ * K[nnzb][S][3][3] (the K output of OptimizedSolidAssembleWithDamping,
+ * optimizedSolidAssemble.pyx:365-431).  Deterministic: one launch per colour.
+ *   kt_full device f64 [E][81]; coef device f64 [E][S];
+ *   block_pos device int32 [E][9] (CSR slot of block (a,b) of element e);
+ *   color_ptr host int64 [n_colors+1], color_elems device int32 [E].
+ * K must be zeroed by the caller (it accumulates, like the reference).        */
+int cvfes_solid_assemble_bsr_f64(int64_t n_elems, int64_t n_samples, const double* kt_full,
+                                 const double* coef, const int32_t* block_pos,
+                                 int32_t n_colors, const int64_t* color_ptr,
+                                 const int32_t* color_elems, double* K, void* stream);
+
+/* ------------------------------------------------------------ the hot path
+ * res += K v for the reference block-CSR layout (MultiplyByVector,
+ * optimizedSolidAssemble.pyx:1250-1274): indptr/indices device int64,
+ * K f64 [nnzb][S][3][3], v and res f64 [3N][S].                               */
+int cvfes_bsr_spmv_f64(int64_t n_nodes, int64_t n_samples, const int64_t* indptr,
+                       const int64_t* indices, const double* K, const double* v,
+                       double* res, void* stream);
+
+/* res = K_s u_s  (+ res if accumulate) from the element templates, all samples
+ * (the per-step Ku of assemble_K_P, physicsSolverSDampGPUs.cl:232-393, and
+ * MultiplyByVector on the assembled matrix, in template form).                */
+int cvfes_solid_kmul_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                         const double* u, double* res, int32_t accumulate, void* stream);
+int cvfes_solid_kmul_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                         const float* u, float* res, int32_t accumulate, void* stream);
+
+/* One explicit damped step for all samples (replaces assemble_K_P + calc_u +
+ * host Dirichlet + calc_u_appTrac, physicsSolverSDampGPUs.py:325-399, and
+ * SolidSolver.Solve, physicsSolver.py:263-292):
+ *   u_next = ( dt^2 (p*fhat - K u) + 2 m u + (dt/2*damp*m - m) u_prev ) / (m (1 + dt/2*damp))
+ *   Dirichlet rows of u_next = clamp_value; rows with m == 0 give 0.
+ * Pressure is p_sched[clock[0] + j] (device f64 schedule, device int64 clock)
+ * or, when p_sched is NULL, the value `pressure`.  trac (device T [N][4] or
+ * NULL) adds an external nodal traction dt^2 * trac / (m (1+dt/2 damp))
+ * (calc_u_appTrac, physicsSolverSDampGPUs.cl:436-446).                        */
+int cvfes_solid_step_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
+                         const double* u, const double* u_prev, double* u_next,
+                         const double* p_sched, const int64_t* clock, int64_t j,
+                         double pressure, const double* trac, double dt, double damp,
+                         void* stream);
+int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef, const float* invm,
+                         const float* u, const float* u_prev, float* u_next,
+                         const double* p_sched, const int64_t* clock, int64_t j,
+                         double pressure, const float* trac, double dt, double damp,
+                         void* stream);
+
+/* n_steps steps with the buffer rotation (u_next, u, u_prev) <- (u_prev, u_next, u)
+ * of physicsSolverSDampGPUs.py:398-399.  bufs[0] = u_n, bufs[1] = u_{n-1},
+ * bufs[2] = free on entry; on return *rot tells which: u_n is bufs[(rot+0)%3]...
+ * precisely, after k steps u_n is bufs[(3 - k % 3) % 3] — returned as *cur_idx,
+ * u_{n-1} as *prev_idx.  After the steps the clock (if given) advances by n_steps. */
+int cvfes_solid_advance_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
+                            double* buf0, double* buf1, double* buf2,
+                            const double* p_sched, int64_t* clock, int64_t n_steps,
+                            double dt, double damp, int32_t* cur_idx, int32_t* prev_idx,
+                            void* stream);
+int cvfes_solid_advance_f32(const cvfes_solid_mesh* mesh, const float* coef, const float* invm,
+                            float* buf0, float* buf1, float* buf2,
+                            const double* p_sched, int64_t* clock, int64_t n_steps,
+                            double dt, double damp, int32_t* cur_idx, int32_t* prev_idx,
+                            void* stream);
+
+/* Initial state u_{-1} = u0 - dt du0 + dt^2/2 ddu0 with ddu0 = (p0 fhat - damp m du0 - K u0)/m
+ * (LocalInitialize, physicsSolver.py:209-230; calc_ddu, physicsSolverSDampGPUs.cl:398-409).
+ * u0, du0 device T [3N][S]; writes u_prev.  Uses `work` T [3N][S] for K u0.  */
+int cvfes_solid_init_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
+                         const double* u0, const double* du0, double* u_prev, double* work,
+                         double p0, double dt, double damp, void* stream);
+int cvfes_solid_init_f32(const cvfes_solid_mesh* mesh, const float* coef, const float* invm,
+                         const float* u0, const float* du0, float* u_prev, float* work,
+                         double p0, double dt, double damp, void* stream);
+
+/* FP64 per-sample norms and the NaN/Inf watchdog (no reference counterpart;
+ * the reference only prints wall-clock timers, solver.py:112-131).
+ *   out f64 [S][4]: sum u^2, sum (u-u_prev)^2, sum m (u-u_prev)^2 (m from invm),
+ *                   count of non-finite values.
+ *   work f64, at least cvfes_norms_work_size(N, S) doubles (block partials).
+ * Returns CVFES_ERR_NONFINITE (after writing out) when any value is NaN/Inf
+ * and check_finite != 0 (this synchronises the stream).                       */
+int64_t cvfes_norms_work_size(int64_t n_nodes, int64_t n_samples);
+int cvfes_solid_norms_f64(int64_t n_nodes, int64_t n_samples, const double* u,
+                          const double* u_prev, const double* invm, double* work,
+                          double* out, int32_t check_finite, void* stream);
+int cvfes_solid_norms_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                          const float* u_prev, const float* invm, double* work,
+                          double* out, int32_t check_finite, void* stream);
+
+/* ------------------------------------------------------------ CUDA graphs
+ * Capture `chunk` steps of cvfes_solid_advance (chunk a multiple of 3 so the
+ * buffer roles repeat) plus the clock increment into one executable graph.
+ * Each cvfes_graph_launch advances `chunk` steps.  precision: 32 or 64.       */
+typedef struct cvfes_graph cvfes_graph;
+int cvfes_graph_capture_advance(const cvfes_solid_mesh* mesh, int32_t precision,
+                                const void* coef, const void* invm,
+                                void* buf0, void* buf1, void* buf2,
+                                const double* p_sched, int64_t* clock, int64_t chunk,
+                                double dt, double damp, void* stream, cvfes_graph** out);
+int cvfes_graph_launch(cvfes_graph* g, void* stream);
+int cvfes_graph_destroy(cvfes_graph* g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVFES_B200_H */

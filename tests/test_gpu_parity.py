@@ -1,0 +1,206 @@
+"""Parity of the sm_100a solid path with the CPU oracle (the reference's own kernels).
+
+Tolerances (relative L2 of displacement unless stated):
+* FP64 form vs the FP64 oracle: <= 1e-12;
+* FP32-state form vs the FP64 oracle: <= 1e-5;
+* one-time FP64 set-up arrays (templates, mass, load, assembled blocks): <= 1e-13 max-relative.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from cvfes_b200 import _lib
+from cvfes_b200._lib import call, ptr
+from cvfes_b200.mesh import SolidMesh
+from cvfes_b200.plan import SolidPlan, color_greedy
+from cvfes_b200.solver import GPUSolidSolver, LocalComm
+from oracle import solid_oracle as so
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+FP64_TOL = 1e-12
+FP32_TOL = 1e-5
+
+
+class Cfg:
+    def __init__(self, dt, nSmp, precision=64, **kw):
+        self.dt = dt
+        self.nSmp = nSmp
+        self.gpu = type("G", (), dict(precision=precision, use_graph=True, graph_chunk=kw.get("chunk", 6),
+                                      watchdog=True, device=0))()
+        self.dt_f = 0.01
+        self.exportBdyStressFilename = None
+        self.useConstantStress = False
+        self.constant_T = 1.0
+        self.constant_pressure = 0.0
+        self.pressure_ramp = "linear"
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLD, name)))
+
+
+def golden_mesh(g, **kw):
+    return SolidMesh(g["nodes"], g["elements"], g["boundary"], g["coefK"].shape[1],
+                     density=float(g["density"]), v=float(g["v"]), damp=float(g["damp"]),
+                     coefK=g["coefK"], gthick=g["gthick"])
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max())
+
+
+@pytest.mark.parametrize("name", ["tube8x6_element.npz", "tube6x5_nodal.npz"])
+def test_setup_kernels_match_reference_assembly(lib, cuda, name):
+    """Templates, lumped mass, unit load and block-CSR assembly vs the reference's outputs."""
+    g = golden(name)
+    nodes, elems = g["nodes"], g["elements"]
+    N, E, S = len(nodes), len(elems), g["coefK"].shape[1]
+    plan = SolidPlan(nodes, elems, 0, 0.0, float(g["v"]), float(g["density"]), cuda,
+                     precisions=(32, 64), keep_full=True)
+    plan.set_material(g["coefK"], g["gthick"])
+    Kt, T, area = so.element_templates(nodes, elems, float(g["v"]))
+    assert rel(plan.kt_full.view(E, 9, 9).cpu().numpy(), Kt) < 1e-13
+    assert rel(plan.area.cpu().numpy(), area) < 1e-14
+    lm = plan.lm.cpu().numpy()
+    assert rel(np.repeat(lm, 3, axis=0), g["LM"]) < 1e-13
+    fh = plan.fhat64.cpu().numpy()[:, :3].ravel()
+    assert rel(fh, g["f"]) < 1e-13
+    # block-CSR assembly in the reference layout, one launch per colour
+    colors, nc = color_greedy(elems, N)
+    order = np.argsort(colors, kind="stable").astype(np.int32)
+    cptr = np.zeros(nc + 1, dtype=np.int64)
+    cptr[1:] = np.cumsum(np.bincount(colors, minlength=nc))
+    pos = so.block_positions(g["indptr"], g["indices"], elems).reshape(E, 9).astype(np.int32)
+    K = torch.zeros((len(g["indices"]), S, 3, 3), dtype=torch.float64, device=cuda)
+    pos_d = torch.from_numpy(pos).to(cuda)
+    order_d = torch.from_numpy(order).to(cuda)
+    call("cvfes_solid_assemble_bsr_f64", E, S, ptr(plan.kt_full), ptr(plan.coef64), ptr(pos_d),
+         nc, ptr(cptr), ptr(order_d), ptr(K), torch.cuda.current_stream().cuda_stream)
+    assert rel(K.cpu().numpy(), g["K"]) < 1e-13
+    # and the reference-layout SpMV on it
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal((3 * N, S))
+    res = torch.zeros((3 * N, S), dtype=torch.float64, device=cuda)
+    ip = torch.from_numpy(g["indptr"]).to(cuda)
+    ix = torch.from_numpy(g["indices"]).to(cuda)
+    vd = torch.from_numpy(v).to(cuda)
+    call("cvfes_bsr_spmv_f64", N, S, ptr(ip), ptr(ix), ptr(K), ptr(vd), ptr(res),
+         torch.cuda.current_stream().cuda_stream)
+    ref = so.multiply_by_vector(g["indptr"], g["indices"], g["K"], v)
+    assert rel(res.cpu().numpy(), ref) < 1e-13
+    # template K*u equals the assembled block-CSR K*u
+    d64 = plan.desc(64)
+    out = torch.empty_like(res)
+    call("cvfes_solid_kmul_f64", _lib.C.byref(d64), ptr(plan.coef64), ptr(vd), ptr(out), 0,
+         torch.cuda.current_stream().cuda_stream)
+    assert rel(out.cpu().numpy(), ref) < 1e-13
+    d32 = plan.desc(32)
+    v32 = vd.float()
+    out32 = torch.empty_like(v32)
+    call("cvfes_solid_kmul_f32", _lib.C.byref(d32), ptr(plan.coef32), ptr(v32), ptr(out32), 0,
+         torch.cuda.current_stream().cuda_stream)
+    assert rel(out32.double().cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["tube8x6_element.npz", "tube6x5_nodal.npz"])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_solver_class_reproduces_golden_history(lib, cuda, name, precision):
+    """GPUSolidSolver.Solve step by step against the reference kernels' history."""
+    g = golden(name)
+    mesh = golden_mesh(g)
+    solver = GPUSolidSolver(LocalComm(), mesh, Cfg(float(g["dt"]), mesh.nSmp, precision))
+    tol = FP64_TOL if precision == 64 else FP32_TOL
+    k = 0
+    for n, p in enumerate(g["pressures"]):
+        solver.pressure = float(p)
+        solver.Solve(n * float(g["dt"]), float(g["dt"]))
+        if (n + 1) % 5 == 0:
+            assert so.rel_l2(solver.displacement(), g["hist"][k]) < tol
+            k += 1
+    assert k == len(g["hist"])
+
+
+def c0_mesh(S=8):
+    from cvfes_b200.cases import CASES, build_mesh
+    return build_mesh(CASES["tube64x128"], n_samples=S)
+
+
+@pytest.fixture(scope="module")
+def c0_oracle():
+    """FP64 oracle history of the 64x128 tube, 8 samples, 400 steps (every 50 steps)."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh()
+    coefK, gthick = mesh.element_coefficients()
+    backend = "reference" if so.load_reference_module() is not None else "numpy"
+    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
+                             mesh.density, mesh.v, mesh.damp, case.dt, backend=backend)
+    hist = o.run(case.pressures(), history_every=50)
+    return mesh, case, hist, backend
+
+
+@pytest.mark.parametrize("precision,use_graph", [(64, True), (64, False), (32, True)])
+def test_tube64x128_400_steps(lib, cuda, c0_oracle, precision, use_graph):
+    """The 64x128 tube, 8 samples, 400 steps: FP64 <= 1e-12, FP32 <= 1e-5 at every 50th step."""
+    mesh, case, hist, backend = c0_oracle
+    cfg = Cfg(case.dt, mesh.nSmp, precision, chunk=24)
+    solver = GPUSolidSolver(LocalComm(), mesh, cfg)
+    pres = case.pressures()
+    worst = 0.0
+    for k in range(8):
+        solver.Advance(pres[50 * k:50 * (k + 1)], use_graph=use_graph)
+        err = so.rel_l2(solver.displacement(), hist[k])
+        worst = max(worst, err)
+    tol = FP64_TOL if precision == 64 else FP32_TOL
+    print(f"precision={precision} graph={use_graph} oracle={backend} max rel-L2 = {worst:.3e}")
+    assert worst < tol
+
+
+def test_graph_replay_is_bitwise_equal_to_plain_launches(lib, cuda):
+    mesh = c0_mesh(4)
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    out = []
+    for use_graph in (True, False):
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 4, 32, chunk=12))
+        s.Advance(case.pressures(100), use_graph=use_graph)
+        out.append(s.local_displacement().clone())
+    assert torch.equal(out[0], out[1])
+
+
+def test_norms_and_watchdog(lib, cuda):
+    mesh = c0_mesh(4)
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 4, 64))
+    s.Advance(case.pressures(150))
+    nrm = s.Norms()
+    u = s.bufs[s.cur].cpu().numpy()
+    up = s.bufs[s.prev].cpu().numpy()
+    m = np.repeat(s.plan.lm.cpu().numpy(), 3, axis=0)
+    assert np.allclose(nrm[:, 0], (u ** 2).sum(0), rtol=1e-12)
+    assert np.allclose(nrm[:, 1], ((u - up) ** 2).sum(0), rtol=1e-12)
+    assert np.allclose(nrm[:, 2], (m * (u - up) ** 2).sum(0), rtol=1e-10)
+    assert np.all(nrm[:, 3] == 0)
+    # a NaN planted in a host buffer and uploaded into the state trips the watchdog
+    bad = u.copy()
+    bad[100, 2] = np.nan
+    s.bufs[s.cur].copy_(torch.from_numpy(bad))
+    with pytest.raises(_lib.NonFiniteError):
+        s.Norms()
+    assert s.Norms(check_finite=False)[2, 3] == 1
+
+
+def test_invalid_arguments_are_rejected(lib, cuda):
+    mesh = c0_mesh(4)
+    s = GPUSolidSolver(LocalComm(), mesh, Cfg(2e-6, 4, 64))
+    with pytest.raises(_lib.CvfesError):
+        call("cvfes_solid_step_f64", _lib.C.byref(s._desc), None, None, None, None, None, None,
+             None, 0, 0.0, None, 2e-6, 0.0, None)
+    with pytest.raises(_lib.CvfesError):
+        call("cvfes_solid_step_f64", _lib.C.byref(s._desc), ptr(s.plan.coef64),
+             ptr(s.plan.invm64), ptr(s.bufs[0]), ptr(s.bufs[1]), ptr(s.bufs[2]), None, None, 0,
+             0.0, None, -1.0, 0.0, None)
