@@ -43,6 +43,8 @@ class SolidMeshDesc(C.Structure):
         ("slot_rec", C.c_void_p),
         ("slot_k", C.c_void_p),
         ("fhat", C.c_void_p),
+        ("max_degree", C.c_int64),
+        ("status", C.c_void_p),
     ]
 
 
@@ -79,7 +81,20 @@ SIGNATURES = {
                                               C.POINTER(C.c_void_p)]),
     "cvfes_graph_launch": (C.c_int, [P, P]),
     "cvfes_graph_destroy": (C.c_int, [P]),
+    "cvfes_set_step_tuning": (C.c_int, [I32, I32, I32, I32, I32]),
+    "cvfes_get_step_tuning": (C.c_int, [I32, P, P, P, P]),
+    "cvfes_status_read": (C.c_int, [P, P]),
 }
+
+
+def get_step_tuning(precision: int) -> dict:
+    vals = [C.c_int32() for _ in range(4)]
+    call("cvfes_get_step_tuning", precision, *[C.byref(v) for v in vals])
+    return dict(zip(("vec", "npb", "staged", "minb"), (v.value for v in vals)))
+
+
+def set_step_tuning(precision: int, vec: int, npb: int, staged: int, minb: int) -> None:
+    call("cvfes_set_step_tuning", precision, vec, npb, staged, minb)
 
 _lock = threading.Lock()
 _lib = None

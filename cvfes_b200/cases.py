@@ -53,6 +53,7 @@ class TubeCase:
     damp: float = 100.0
     tau: float = 0.1
     marginal: str = "exact"
+    mass_lumping: str = "reference"
     extra: dict = field(default_factory=dict)
 
     def geometry(self) -> TubeGeometry:
@@ -66,7 +67,14 @@ class TubeCase:
 
 CASES = {
     "tube64x128": TubeCase("tube64x128", 64, 128, 3.0, n_samples=8, dt=2e-6, n_steps=400),
-    "tube256x1024": TubeCase("tube256x1024", 256, 1024, 3.0, n_samples=512, dt=5e-7, n_steps=2000),
+    # dt = 5e-7 exceeds the stability limit of the reference's lumped mass on this mesh
+    # (power iteration: dt_crit 3.8e-7 .. 4.3e-7 over the 512 samples); with row-sum
+    # lumping (3x that mass) dt_crit is 6.6e-7 .. 7.4e-7 and the step is stable.
+    "tube256x1024": TubeCase("tube256x1024", 256, 1024, 3.0, n_samples=512, dt=5e-7,
+                             n_steps=2000, mass_lumping="rowsum"),
+    # half-length refinement used for kernel profiles: 1.2 GB of state, still 10x L2
+    "tube256x512": TubeCase("tube256x512", 256, 512, 1.5, n_samples=256, dt=5e-7, n_steps=1000,
+                            mass_lumping="rowsum"),
     "adjoint64": TubeCase("adjoint64", 64, 128, 3.0, n_samples=64, dt=2e-6, n_steps=500,
                           extra=dict(n_obs=512, obs_every=10, ckpt_every=50)),
     "stenosed512x2048": TubeCase("stenosed512x2048", 512, 2048, 5.0, stenosed=True,
@@ -100,7 +108,7 @@ def build_mesh(case: TubeCase, n_samples: Optional[int] = None, cache: bool = Tr
             np.savez(path, elmE=elmE, elmThick=elmH)
     return SolidMesh(nodes=nodes, elementNodeIds=elems, boundary=np.concatenate([inlet, outlet]),
                      nSmp=S, density=case.density, v=case.nu, damp=case.damp, bdyU=0.0,
-                     elmE=elmE, elmThick=elmH, name=case.name)
+                     elmE=elmE, elmThick=elmH, name=case.name, mass_lumping=case.mass_lumping)
 
 
 def case_dt(case: TubeCase, mesh: SolidMesh) -> float:

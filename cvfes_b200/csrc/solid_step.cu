@@ -53,7 +53,80 @@ struct StepArgs {
     T clamp;
     T eta;
     T w0;
+    int tpn;
+    int npb;
+    int cap_slots;   // slot capacity of the shared-memory stage (staged kernel)
+    int* status;     // bit 0: a bounded wait gave up
 };
+
+// ------------------------------------------------------------ TMA / mbarrier helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+// One-dimensional TMA bulk copy global -> this CTA's shared memory (no multicast).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.b32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after max_polls try_wait rounds (each round suspends the
+// thread for a bounded, hardware-chosen time), so a lost transfer cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase, int max_polls) {
+    for (int i = 0; i < max_polls; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+constexpr int kMaxPolls = 1 << 22;
+
+// Thread -> (node, sample vector).  A block holds `npb` consecutive nodes and
+// `tpn` consecutive sample vectors of each (tpn = min(S/VEC, 32)); blockIdx.y
+// picks the sample chunk.  The warps of one block therefore gather overlapping
+// neighbour rows and element coefficients of one sample chunk.
+__device__ __forceinline__ bool map_row(int tpn, int npb, long long n_nodes, long long& a,
+                                        int& vec) {
+    const int t = threadIdx.x / tpn;
+    if (t >= npb) return false;
+    a = (long long)blockIdx.x * npb + t;
+    vec = blockIdx.y * tpn + (threadIdx.x - t * tpn);
+    return a < n_nodes;
+}
+
+struct RowGrid {
+    dim3 grid;
+    int tpn, npb;
+};
+
+inline RowGrid row_grid(long long n_nodes, int sv, int block) {
+    RowGrid g;
+    g.tpn = sv < 32 ? sv : 32;
+    g.npb = block / g.tpn;
+    g.grid = dim3((unsigned)((n_nodes + g.npb - 1) / g.npb), (unsigned)(sv / g.tpn));
+    return g;
+}
 
 // Row a of K_s u_s for VEC samples starting at column col.
 template <typename T, int V, bool DIFF>
@@ -127,27 +200,11 @@ __device__ __forceinline__ void ku_row(const int32_t* __restrict__ node_ptr,
     }
 }
 
-template <typename T, int V, bool DIFF>
-__global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
-    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int SV = A.S / V;
-    const long long a = g / SV;
-    if (a >= A.n_nodes) return;
-    const size_t S = (size_t)A.S;
-    const size_t col = (size_t)(g - a * SV) * V;
-    const size_t row = (size_t)a * 3 * S + col;
-    if (a < A.n_clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
-        return;
-    }
-    Vec<T, V> ua[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
-    Vec<T, V> acc[3];
-    ku_row<T, V, DIFF>(A.node_ptr, A.rec, A.slab, A.coef, A.u, S, col, a, ua, acc);
-
+// Fused update of one node row (increment form, see the file header) and its store.
+template <typename T, int V>
+__device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
+                                              size_t col, size_t row, const Vec<T, V> (&ua)[3],
+                                              const Vec<T, V> (&acc)[3]) {
     const double pd = A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure;
     const T p = (T)pd;
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
@@ -170,15 +227,172 @@ __global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
 }
 
 template <typename T, int V, bool DIFF>
+__global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
+    long long a;
+    int vec;
+    if (!map_row(A.tpn, A.npb, A.n_nodes, a, vec)) return;
+    const size_t S = (size_t)A.S;
+    const size_t col = (size_t)vec * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    if (a < A.n_clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    Vec<T, V> ua[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
+    Vec<T, V> acc[3];
+    ku_row<T, V, DIFF>(A.node_ptr, A.rec, A.slab, A.coef, A.u, S, col, a, ua, acc);
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc);
+}
+
+// ------------------------------------------------------------ TMA-staged step
+// Row a of K_s u_s with the node's slot records and stiffness rows read from
+// shared memory; the gathers of element k+1 are issued before element k is
+// multiplied, so two elements' loads are in flight per warp.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row_staged(const int4* srec, const T* sslab, int k0, int k1,
+                                              const T* __restrict__ u, const T* __restrict__ coef,
+                                              size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                              Vec<T, V> (&acc)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    if (k0 >= k1) return;
+    int4 r = srec[k0];
+    Vec<T, V> x1[3], x2[3], c;
+    {
+        const T* p1 = u + (size_t)r.y * 3 * S + col;
+        const T* p2 = u + (size_t)r.z * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x1[d] = ldg<T, V>(p1 + d * S);
+            x2[d] = ldg<T, V>(p2 + d * S);
+        }
+        c = ldg<T, V>(coef + (size_t)r.x * S + col);
+    }
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        const bool more = k + 1 < k1;
+        int4 rn = r;
+        Vec<T, V> x2n[3], cn;
+        if (more) {
+            rn = srec[k + 1];
+            const T* p2 = u + (size_t)rn.z * 3 * S + col;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x2n[d] = ldg<T, V>(p2 + d * S);
+            cn = ldg<T, V>(coef + (size_t)rn.x * S + col);
+        }
+        const T* K = sslab + (size_t)kSlabStride * k;
+        Vec<T, V> d1[3], d2[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            d1[d] = DIFF ? vsub(x1[d], ua[d]) : x1[d];
+            d2[d] = DIFF ? vsub(x2[d], ua[d]) : x2[d];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            Vec<T, V> t = vzero<T, V>();
+            if constexpr (!DIFF) {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) axpy(t, K[3 * i + jj], ua[jj]);
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, K[9 + 3 * i + jj], d1[jj]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, K[18 + 3 * i + jj], d2[jj]);
+            vfma(acc[i], c, t);
+        }
+        if (more) {
+            if (rn.w & 1) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) x1[d] = x2[d];
+            } else {
+                const T* p1 = u + (size_t)rn.y * 3 * S + col;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) x1[d] = ldg<T, V>(p1 + d * S);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x2[d] = x2n[d];
+            c = cn;
+            r = rn;
+        }
+    }
+}
+
+// One warp per node and 32*VEC samples of it; a block holds npb consecutive nodes
+// of one sample chunk (blockIdx.y).  Thread 0 stages the block's slot records and
+// stiffness rows with two TMA bulk copies while every warp loads its node's own
+// displacement and prefetches its epilogue rows into L2.
+template <typename T, int V, bool DIFF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long a0 = (long long)blockIdx.x * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots) {  // cannot happen when cap_slots = npb * max_degree
+        if (threadIdx.x == 0 && A.status) atomicOr(A.status, 2);
+        return;
+    }
+    const uint32_t bar = smem_u32(smem);
+    int4* srec = reinterpret_cast<int4*>(smem + 16);
+    T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_rec = (uint32_t)nsl * 16u;
+        const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        if (nsl > 0) {
+            bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+            bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+        }
+    }
+    const long long a = a0 + warp;
+    const bool active = warp < A.npb && a < a1;
+    const size_t S = (size_t)A.S;
+    const size_t col = ((size_t)blockIdx.y * 32 + lane) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    const bool clamped = a < A.n_clamped;
+    Vec<T, V> ua[3];
+    if (active && !clamped) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ua[d] = ldg<T, V>(A.u + row + d * S);
+            prefetch_l2(A.up + row + d * S);
+        }
+        prefetch_l2(A.invm + (size_t)a * S + col);
+    }
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        if (lane == 0 && A.status) atomicOr(A.status, 1);
+        return;
+    }
+    if (!active) return;
+    if (clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    Vec<T, V> acc[3];
+    const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+    ku_row_staged<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc);
+}
+
+template <typename T, int V, bool DIFF>
 __global__ void __launch_bounds__(256)
     k_kmul(const int32_t* node_ptr, const int4* rec, const T* slab, const T* coef, const T* u,
-           T* res, long long n_nodes, int S_, int accumulate) {
-    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int SV = S_ / V;
-    const long long a = g / SV;
-    if (a >= n_nodes) return;
+           T* res, long long n_nodes, int S_, int accumulate, int tpn, int npb) {
+    long long a;
+    int vec;
+    if (!map_row(tpn, npb, n_nodes, a, vec)) return;
     const size_t S = (size_t)S_;
-    const size_t col = (size_t)(g - a * SV) * V;
+    const size_t col = (size_t)vec * V;
     const size_t row = (size_t)a * 3 * S + col;
     Vec<T, V> ua[3], acc[3];
 #pragma unroll
@@ -314,6 +528,45 @@ int check_mesh(const cvfes_solid_mesh* m, const char* who) {
     return CVFES_OK;
 }
 
+struct StepTuning {
+    int vec;
+    int npb;
+    int staged;
+    int minb;  // minimum resident blocks per SM asked of the compiler (register cap)
+};
+// Defaults from a sweep on the 256x1024 tube with 512 samples (B200).
+static StepTuning g_tune32 = {4, 4, 1, 2};
+static StepTuning g_tune64 = {2, 4, 1, 2};
+template <typename T>
+StepTuning& tuning_of() {
+    return sizeof(T) == 4 ? g_tune32 : g_tune64;
+}
+constexpr size_t kMaxStageBytes = 160 * 1024;
+
+template <typename K, typename A_>
+int launch_staged(K kernel, dim3 grid, int threads, size_t smem, cudaStream_t st, const A_& A) {
+    if (smem > 48 * 1024) {
+        cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return fail(CVFES_ERR_CUDA, "k_step_staged smem attribute: %s", cudaGetErrorString(e));
+    }
+    kernel<<<grid, threads, smem, st>>>(A);
+    CVFES_LAUNCH_CHECK("k_step_staged");
+    return CVFES_OK;
+}
+
+template <typename T, int V, bool DIFF>
+int launch_staged_v(int minb, dim3 grid, int threads, size_t smem, cudaStream_t st,
+                    const StepArgs<T>& A) {
+    switch (minb) {
+        case 4: return launch_staged(k_step_staged<T, V, DIFF, 4>, grid, threads, smem, st, A);
+        case 3: return launch_staged(k_step_staged<T, V, DIFF, 3>, grid, threads, smem, st, A);
+        case 2: return launch_staged(k_step_staged<T, V, DIFF, 2>, grid, threads, smem, st, A);
+        default: return launch_staged(k_step_staged<T, V, DIFF, 1>, grid, threads, smem, st, A);
+    }
+}
+
 template <typename T>
 int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u,
                 const T* up, T* un, const double* p_sched, const long long* clock, long long j,
@@ -345,17 +598,42 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     const double g = 0.5 * dt * damp;
     A.eta = (T)(dt * damp / (1.0 + g));
     A.w0 = (T)(dt * dt / (1.0 + g));
+    A.status = m->status;
+    A.cap_slots = 0;
     const void* ptrs[6] = {coef, invm, u, up, un, nullptr};
-    const int V = pick_vec<T>(ptrs, 5, A.S);
-    const int block = 256;
-    const unsigned grid = grid_1d(m->n_nodes * (A.S / V), block);
+    const StepTuning& tune = tuning_of<T>();
+    int V = pick_vec<T>(ptrs, 5, A.S);
+    while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
+    // TMA-staged kernel: a warp per node needs S/V to be a multiple of 32.
+    const long long cap = (long long)tune.npb * m->max_degree;
+    const size_t smem = 16 + (size_t)cap * (16 + kSlabStride * sizeof(T));
+    if (tune.staged && m->max_degree > 0 && (A.S / V) % 32 == 0 && smem <= kMaxStageBytes) {
+        A.npb = tune.npb;
+        A.tpn = 32;
+        A.cap_slots = (int)cap;
+        const dim3 grid((unsigned)((m->n_nodes + A.npb - 1) / A.npb), (unsigned)(A.S / V / 32));
+        const int threads = 32 * A.npb;
+        if (V == 4) {
+            if constexpr (sizeof(T) == 4)
+                rc = launch_staged_v<T, 4, DIFF>(tune.minb, grid, threads, smem, st, A);
+        } else if (V == 2) {
+            rc = launch_staged_v<T, 2, DIFF>(tune.minb, grid, threads, smem, st, A);
+        } else {
+            rc = launch_staged_v<T, 1, DIFF>(tune.minb, grid, threads, smem, st, A);
+        }
+        return rc;
+    }
+    const int block = 256;
+    const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
+    A.tpn = rg.tpn;
+    A.npb = rg.npb;
     if (V == 4) {
-        if constexpr (sizeof(T) == 4) k_step<T, 4, DIFF><<<grid, block, 0, st>>>(A);
+        if constexpr (sizeof(T) == 4) k_step<T, 4, DIFF><<<rg.grid, block, 0, st>>>(A);
     } else if (V == 2) {
-        k_step<T, 2, DIFF><<<grid, block, 0, st>>>(A);
+        k_step<T, 2, DIFF><<<rg.grid, block, 0, st>>>(A);
     } else {
-        k_step<T, 1, DIFF><<<grid, block, 0, st>>>(A);
+        k_step<T, 1, DIFF><<<rg.grid, block, 0, st>>>(A);
     }
     CVFES_LAUNCH_CHECK("k_step");
     return CVFES_OK;
@@ -371,20 +649,21 @@ int launch_kmul(const cvfes_solid_mesh* m, const T* coef, const T* u, T* res, in
     const void* ptrs[3] = {coef, u, res};
     const int V = pick_vec<T>(ptrs, 3, S);
     const int block = 256;
-    const unsigned grid = grid_1d(m->n_nodes * (S / V), block);
+    const RowGrid rg = row_grid(m->n_nodes, S / V, block);
+    const dim3 grid = rg.grid;
     constexpr bool DIFF = std::is_same<T, float>::value;
     const int4* rec = reinterpret_cast<const int4*>(m->slot_rec);
     const T* slab = static_cast<const T*>(m->slot_k);
     if (V == 4) {
         if constexpr (sizeof(T) == 4)
             k_kmul<T, 4, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
-                                                       m->n_nodes, S, accumulate);
+                                                       m->n_nodes, S, accumulate, rg.tpn, rg.npb);
     } else if (V == 2) {
         k_kmul<T, 2, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
-                                                   m->n_nodes, S, accumulate);
+                                                   m->n_nodes, S, accumulate, rg.tpn, rg.npb);
     } else {
         k_kmul<T, 1, DIFF><<<grid, block, 0, st>>>(m->node_ptr, rec, slab, coef, u, res,
-                                                   m->n_nodes, S, accumulate);
+                                                   m->n_nodes, S, accumulate, rg.tpn, rg.npb);
     }
     CVFES_LAUNCH_CHECK("k_kmul");
     return CVFES_OK;
@@ -624,5 +903,50 @@ extern "C" int cvfes_graph_destroy(cvfes_graph* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
     delete g;
+    return CVFES_OK;
+}
+
+// ------------------------------------------------------------------ tuning, status
+extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb,
+                                     int32_t staged, int32_t minb) {
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: precision must be 32 or 64");
+    const int maxv = precision == 32 ? 4 : 2;
+    if (vec < 1 || vec > maxv || (vec & (vec - 1)))
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: vec must be 1, 2%s",
+                    maxv == 4 ? " or 4" : "");
+    if (npb < 1 || npb > 8)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: npb must be in 1..8");
+    if (minb < 1 || minb > 4)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: minb must be in 1..4");
+    StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
+    t.vec = vec;
+    t.npb = npb;
+    t.staged = staged ? 1 : 0;
+    t.minb = minb;
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb,
+                                     int32_t* staged, int32_t* minb) {
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_get_step_tuning: precision must be 32 or 64");
+    const StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
+    if (vec) *vec = t.vec;
+    if (npb) *npb = t.npb;
+    if (staged) *staged = t.staged;
+    if (minb) *minb = t.minb;
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_status_read(int32_t* status, void* stream) {
+    if (!status) return fail(CVFES_ERR_ARG, "cvfes_status_read: null status");
+    int32_t h = 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    CVFES_CUDA_TRY(cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CVFES_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int32_t), st));
+    CVFES_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h & 1) return fail(CVFES_ERR_TIMEOUT, "a bounded device wait gave up (status %d)", h);
+    if (h) return fail(CVFES_ERR_ARG, "device status %d: slot stage overflow", h);
     return CVFES_OK;
 }

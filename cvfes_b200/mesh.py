@@ -160,6 +160,7 @@ class SolidMesh:
     iniU: Optional[np.ndarray] = None
     iniDu: Optional[np.ndarray] = None
     name: str = "wall"
+    mass_lumping: str = "reference"
     dof: int = 3
     colorGroups: Optional[list] = field(default=None, repr=False)
 

@@ -39,11 +39,19 @@ def d_matrix(v: float, k: float = SHEAR_K) -> np.ndarray:
     return D
 
 
-def lumped_mass_weights(density: float) -> np.ndarray:
-    """mw[a, g] = rho * w_g^2 * N_g(a): row sum of tM_g * w_g for local node a
-    (tM_g = N_gᵀN_g w_g rho, physicsSolver.py:190-197; the assembly multiplies
-    by w_g once more, optimizedSolidAssemble.pyx:564-566)."""
-    return density * (QUAD[:, :3] * (QUAD[:, 3:4] ** 2)).T.copy()
+def lumped_mass_weights(density: float, lumping: str = "reference") -> np.ndarray:
+    """Row-sum weights ``mw[a, g]`` of the lumped mass of local node ``a``.
+
+    ``reference``: ``rho * w_g^2 * N_g(a)`` -- the row sum of ``tM_g * w_g``
+    (``tM_g = N_gᵀN_g w_g rho``, physicsSolver.py:190-197; the assembly applies
+    ``w_g`` a second time, optimizedSolidAssemble.pyx:564-566), one third of
+    the element mass per node.
+    ``rowsum``: ``rho * w_g * N_g(a)`` -- the row sum of the consistent mass
+    matrix (the full rho*h*A/3 per node); equal to ``reference`` with 3 rho."""
+    w = QUAD[:, 3:4] ** 2 if lumping == "reference" else QUAD[:, 3:4]
+    if lumping not in ("reference", "rowsum"):
+        raise ValueError("mass lumping must be 'reference' or 'rowsum'")
+    return density * (QUAD[:, :3] * w).T.copy()
 
 
 def incidence(elements: np.ndarray, n_nodes: int):
@@ -73,7 +81,8 @@ class SolidPlan:
     """
 
     def __init__(self, nodes, elements, n_clamped: int, clamp_value: float, v: float,
-                 density: float, device="cuda", precisions=(32, 64), keep_full=False):
+                 density: float, device="cuda", precisions=(32, 64), keep_full=False,
+                 mass_lumping: str = "reference"):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("SolidPlan needs a CUDA device; there is no CPU path")
@@ -85,9 +94,11 @@ class SolidPlan:
         self.clamp_value = float(clamp_value)
         self.v = float(v)
         self.density = float(density)
+        self.mass_lumping = mass_lumping
         self.precisions = tuple(precisions)
         node_ptr, slot_rec, elem_slot = incidence(elements, self.N)
         self.host_node_ptr, self.host_slot_rec = node_ptr, slot_rec
+        self.max_degree = int(np.max(np.diff(node_ptr))) if self.N > 0 else 0
         dev = self.device
         self.stream = torch.cuda.current_stream(dev)
         self.nodes = torch.from_numpy(nodes).to(dev)
@@ -99,6 +110,7 @@ class SolidPlan:
         self.slot_k64 = torch.empty(SLAB * ns, dtype=torch.float64, device=dev) if 64 in self.precisions else None
         self.slot_k32 = torch.empty(SLAB * ns, dtype=torch.float32, device=dev) if 32 in self.precisions else None
         self.kt_full = torch.empty(self.E * 81, dtype=torch.float64, device=dev) if keep_full else None
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.area = torch.empty(self.E, dtype=torch.float64, device=dev)
         self.normal = torch.empty(3 * self.E, dtype=torch.float64, device=dev)
         D = np.ascontiguousarray(d_matrix(self.v))
@@ -134,7 +146,7 @@ class SolidPlan:
         self.invm32 = torch.empty((self.N, S), dtype=torch.float32, device=dev)
         self.fhat64 = torch.empty((self.N, 4), dtype=torch.float64, device=dev)
         self.fhat32 = torch.empty((self.N, 4), dtype=torch.float32, device=dev)
-        mw = np.ascontiguousarray(lumped_mass_weights(self.density))
+        mw = np.ascontiguousarray(lumped_mass_weights(self.density, self.mass_lumping))
         with torch.cuda.device(dev):
             call("cvfes_solid_mass_load_f64", self.N, self.E, S, ptr(self.node_ptr),
                  ptr(self.slot_rec), ptr(self.area), ptr(self.normal), ptr(gth), n_gauss,
@@ -160,4 +172,9 @@ class SolidPlan:
         if slab is None:
             raise RuntimeError(f"plan was built without FP{precision} templates")
         return _lib.SolidMeshDesc(self.N, self.E, self.S, self.n_clamped, self.clamp_value,
-                                  ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat))
+                                  ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat),
+                                  self.max_degree, ptr(self.status))
+
+    def check_status(self):
+        """Raise if a bounded device wait gave up since the last check (syncs the stream)."""
+        call("cvfes_status_read", ptr(self.status), self._s())

@@ -169,7 +169,8 @@ class GPUSolidSolver(PhysicsSolver):
         with torch.cuda.device(dev):
             self.plan = SolidPlan(m.nodes[self.lclNodeIds], self.lclElmNodeIds,
                                   n_clamped=m.lclNSpecialHead, clamp_value=m.bdyU, v=m.v,
-                                  density=m.density, device=dev, precisions=(self.precision,))
+                                  density=m.density, device=dev, precisions=(self.precision,),
+                                  mass_lumping=getattr(m, "mass_lumping", "reference"))
             coefK, gthick = m.element_coefficients()
             self.plan.set_material(coefK, gthick)
             self._desc = self.plan.desc(self.precision)
@@ -262,9 +263,6 @@ class GPUSolidSolver(PhysicsSolver):
                 key = (chunk, float(dt), self.cur, self.prev, self.nxt, p.data_ptr())
                 g = self._graphs.get(key)
                 if g is None:
-                    for old in self._graphs.values():
-                        call("cvfes_graph_destroy", old)
-                    self._graphs.clear()
                     h = _lib.C.c_void_p()
                     b = self.bufs
                     call("cvfes_graph_capture_advance", C_desc(self._desc), prec,
@@ -336,7 +334,37 @@ class GPUSolidSolver(PhysicsSolver):
             call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
                  ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
                  ptr(self.norm_work), ptr(out), int(bool(chk)), self._stream())
+            self.plan.check_status()
         return out.cpu().numpy()
+
+    def LambdaMax(self, iters: int = 200, seed: int = 0) -> np.ndarray:
+        """Largest eigenvalue of M⁻¹K per sample on the free dofs (FP64 power iteration
+        with the template K*u kernel); the central-difference step is stable for
+        ``dt < 2/sqrt(lambda_max)``."""
+        dev = self.device
+        plan = self.plan
+        if plan.slot_k64 is None or plan.coef64 is None:
+            raise RuntimeError("LambdaMax needs the FP64 templates (precision = fp64)")
+        desc = plan.desc(64)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        with torch.cuda.device(dev):
+            x = torch.randn((self.lclNDof, self.nSmp), dtype=torch.float64, device=dev,
+                            generator=g)
+            nc = 3 * plan.n_clamped
+            x[:nc] = 0
+            y = torch.empty_like(x)
+            invm3 = plan.invm64.repeat_interleave(3, dim=0)
+            lam = torch.zeros(self.nSmp, dtype=torch.float64, device=dev)
+            for _ in range(iters):
+                x /= torch.linalg.vector_norm(x, dim=0, keepdim=True)
+                call("cvfes_solid_kmul_f64", C_desc(desc), ptr(plan.coef64), ptr(x), ptr(y), 0,
+                     self._stream())
+                y *= invm3
+                y[:nc] = 0
+                lam = torch.linalg.vector_norm(y, dim=0)
+                x, y = y, x
+        return lam.cpu().numpy()
 
     def local_displacement(self) -> torch.Tensor:
         """Current displacement (lclNDof, S) on the device, local node order."""

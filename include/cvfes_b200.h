@@ -55,7 +55,28 @@ typedef struct cvfes_solid_mesh {
     const int32_t* slot_rec;      /* [4 * n_slots]    */
     const void*    slot_k;        /* [28 * n_slots] T */
     const void*    fhat;          /* [4 * n_nodes]  T */
+    int64_t        max_degree;    /* max slots of one node (0: unknown -> no smem staging) */
+    int32_t*       status;        /* device int32 or NULL: bit 0 set when a bounded
+                                     device wait gave up (read by cvfes_status_read) */
 } cvfes_solid_mesh;
+
+/* Step-kernel tuning (the autotuner sets these; defaults are FP32 vec 4 and
+ * FP64 vec 2, 8 nodes per block, TMA-staged slot rows).
+ *   precision 32 | 64;  vec: samples per thread (FP32 1|2|4, FP64 1|2);
+ *   npb: nodes per block when a warp owns one node (1..8, one warp each);
+ *   staged: 1 = slot records and stiffness rows staged in shared memory by a
+ *           TMA bulk copy, 0 = read through L1;
+ *   minb: resident blocks per SM the register allocation must allow (1..4).
+ * Applies to launches made after the call (graphs keep what they captured). */
+int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,
+                          int32_t minb);
+int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t* staged,
+                          int32_t* minb);
+
+/* Read and clear the device status word of a mesh descriptor (synchronises the
+ * stream).  Returns CVFES_ERR_TIMEOUT if a bounded device wait gave up since
+ * the last read, else CVFES_OK.                                               */
+int cvfes_status_read(int32_t* status, void* stream);
 
 /* ---------------------------------------------------------------- errors */
 const char* cvfes_last_error(void);
