@@ -50,6 +50,31 @@ __device__ __forceinline__ Vec<T, V> ldg(const T* p) {
     }
     return r;
 }
+// Asynchronous global -> shared copy of BYTES (4, 8 or 16) per thread (LSU path).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src), "n"(BYTES)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// VEC values from shared memory (the caller guarantees VEC*sizeof(T) alignment)
+template <typename T, int V>
+__device__ __forceinline__ Vec<T, V> lds(const unsigned char* p) {
+    return *reinterpret_cast<const Vec<T, V>*>(p);
+}
 template <typename T, int V>
 __device__ __forceinline__ void st(T* p, const Vec<T, V>& x) {
     *reinterpret_cast<Vec<T, V>*>(p) = x;
@@ -116,8 +141,19 @@ __device__ __forceinline__ void vfma(Vec<T, V>& acc, const Vec<T, V>& c, const V
 template <typename T, int V>
 __device__ __forceinline__ Vec<T, V> vsub(const Vec<T, V>& a, const Vec<T, V>& b) {
     Vec<T, V> r;
+    if constexpr (std::is_same<T, float>::value && (V % 2) == 0) {
+        // a - b as one packed FMA per pair: (-1) * b + a, exact like the subtraction
 #pragma unroll
-    for (int i = 0; i < V; ++i) r.v[i] = a.v[i] - b.v[i];
+        for (int i = 0; i < V; i += 2) {
+            float2 q = __ffma2_rn(make_float2(b.v[i], b.v[i + 1]), make_float2(-1.0f, -1.0f),
+                                  make_float2(a.v[i], a.v[i + 1]));
+            r.v[i] = q.x;
+            r.v[i + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) r.v[i] = a.v[i] - b.v[i];
+    }
     return r;
 }
 template <typename T, int V>

@@ -56,6 +56,8 @@ struct StepArgs {
     int tpn;
     int npb;
     int cap_slots;   // slot capacity of the shared-memory stage (staged kernel)
+    int gather_rows; // rows of each warp's gather buffer (gather kernel)
+    int nch;         // sample chunks per node block (staged kernels; 1D grid, chunk fastest)
     int* status;     // bit 0: a bounded wait gave up
 };
 
@@ -200,20 +202,36 @@ __device__ __forceinline__ void ku_row(const int32_t* __restrict__ node_ptr,
     }
 }
 
+// The step's pressure: one value per launch, so it is read once at kernel entry
+// (a schedule entry indexed by the device clock, or the value passed by the host).
+template <typename T>
+__device__ __forceinline__ T step_pressure(const StepArgs<T>& A) {
+    return (T)(A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure);
+}
+
+// Nodal external load p*fhat (+ traction) of node a, read early by the caller.
+template <typename T>
+__device__ __forceinline__ void node_load(const StepArgs<T>& A, long long a, T p, T (&f)[3]) {
+    const float4* q = nullptr;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) f[d] = p * __ldg(A.fhat + 4 * a + d);
+    if (A.trac) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) f[d] += __ldg(A.trac + 4 * a + d);
+    }
+    (void)q;
+}
+
 // Fused update of one node row (increment form, see the file header) and its store.
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
-                                              const Vec<T, V> (&acc)[3]) {
-    const double pd = A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure;
-    const T p = (T)pd;
+                                              const Vec<T, V> (&acc)[3], const T (&f)[3]) {
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
-    const T* fh = A.fhat + 4 * a;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const Vec<T, V> up = ldcs<T, V>(A.up + row + d * S);
-        T load = p * __ldg(fh + d);
-        if (A.trac) load += __ldg(A.trac + 4 * a + d);
+        const T load = f[d];
         Vec<T, V> o;
 #pragma unroll
         for (int i = 0; i < V; ++i) {
@@ -243,9 +261,11 @@ __global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
     Vec<T, V> ua[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
+    T f[3];
+    node_load<T>(A, a, step_pressure<T>(A), f);
     Vec<T, V> acc[3];
     ku_row<T, V, DIFF>(A.node_ptr, A.rec, A.slab, A.coef, A.u, S, col, a, ua, acc);
-    step_epilogue<T, V>(A, a, S, col, row, ua, acc);
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
 }
 
 // ------------------------------------------------------------ TMA-staged step
@@ -359,6 +379,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
     const size_t row = (size_t)a * 3 * S + col;
     const bool clamped = a < A.n_clamped;
     Vec<T, V> ua[3];
+    T f[3];
     if (active && !clamped) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -366,6 +387,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
             prefetch_l2(A.up + row + d * S);
         }
         prefetch_l2(A.invm + (size_t)a * S + col);
+        node_load<T>(A, a, step_pressure<T>(A), f);
     }
     if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
         if (lane == 0 && A.status) atomicOr(A.status, 1);
@@ -381,7 +403,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
     Vec<T, V> acc[3];
     const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
     ku_row_staged<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
-    step_epilogue<T, V>(A, a, S, col, row, ua, acc);
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
 }
 
 template <typename T, int V, bool DIFF>
@@ -453,6 +475,573 @@ __global__ void k_bsr_spmv(long long n_nodes, int S, const long long* __restrict
 }
 
 __global__ void k_clock_add(long long* clock, long long n) { clock[0] += n; }
+
+// ------------------------------------------------------------ fan-rotation step
+// The fan order makes the first neighbour of element k the second neighbour of
+// element k-1, so element k needs only one new neighbour row set.  Three register
+// buffers rotate through the roles (previous = first neighbour, current = second
+// neighbour, next = in flight); the slot loop is unrolled three times so the
+// rotation is a renaming, not a copy.  Neighbour rows are turned into differences
+// u_b - u_a once (FP32 form) and reused by the following element.
+template <typename T, int V>
+__device__ __forceinline__ void load_rows(Vec<T, V> (&x)[3], const T* __restrict__ u, int node,
+                                          size_t S, size_t col) {
+    const T* p = u + (size_t)node * 3 * S + col;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] = ldg<T, V>(p + d * S);
+}
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void to_diff(Vec<T, V> (&x)[3], const Vec<T, V> (&ua)[3]) {
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d] = vsub(x[d], ua[d]);
+    }
+}
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void slot_fma(const T* K, const Vec<T, V>& c, const Vec<T, V> (&d1)[3],
+                                         const Vec<T, V> (&d2)[3], const Vec<T, V> (&ua)[3],
+                                         Vec<T, V> (&acc)[3]) {
+    T kk[28];
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int q = (DIFF ? 2 : 0); q < 7; ++q) {
+            const float4 t = reinterpret_cast<const float4*>(K)[q];
+            kk[4 * q] = t.x;
+            kk[4 * q + 1] = t.y;
+            kk[4 * q + 2] = t.z;
+            kk[4 * q + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = (DIFF ? 4 : 0); q < 14; ++q) {
+            const double2 t = reinterpret_cast<const double2*>(K)[q];
+            kk[2 * q] = t.x;
+            kk[2 * q + 1] = t.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Vec<T, V> t = vzero<T, V>();
+        if constexpr (!DIFF) {
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], d1[jj]);
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], d2[jj]);
+        vfma(acc[i], c, t);
+    }
+}
+
+// One element of the fan: prev holds the first neighbour (difference), cur the
+// second one as loaded; the next element's row set is issued into nxt first.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void fan_phase(int& k, int k1, const int4* srec, const T* sslab,
+                                          const T* __restrict__ u, const T* __restrict__ coef,
+                                          size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                          Vec<T, V> (&acc)[3], Vec<T, V> (&prev)[3],
+                                          Vec<T, V> (&cur)[3], const Vec<T, V>& ccur,
+                                          Vec<T, V> (&nxt)[3], Vec<T, V>& cnxt) {
+    const bool more = k + 1 < k1;
+    int4 rn = make_int4(0, 0, 0, 1);
+    if (more) {
+        rn = srec[k + 1];
+        load_rows<T, V>(nxt, u, rn.z, S, col);
+        cnxt = ldg<T, V>(coef + (size_t)rn.x * S + col);
+    }
+    to_diff<T, V, DIFF>(cur, ua);
+    slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, prev, cur, ua, acc);
+    if (more && !(rn.w & 1)) {  // fan break: the next element's first neighbour is new
+        load_rows<T, V>(cur, u, rn.y, S, col);
+        to_diff<T, V, DIFF>(cur, ua);
+    }
+    ++k;
+}
+
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row_fan(const int4* srec, const T* sslab, int k0, int k1,
+                                           const T* __restrict__ u, const T* __restrict__ coef,
+                                           size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                           Vec<T, V> (&acc)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    if (k0 >= k1) return;
+    Vec<T, V> B0[3], B1[3], B2[3], c0, c1, c2;
+    const int4 r0 = srec[k0];
+    load_rows<T, V>(B0, u, r0.y, S, col);
+    load_rows<T, V>(B1, u, r0.z, S, col);
+    c1 = ldg<T, V>(coef + (size_t)r0.x * S + col);
+    to_diff<T, V, DIFF>(B0, ua);
+    int k = k0;
+    while (true) {
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B0, B1, c1, B2, c2);
+        if (k >= k1) break;
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B1, B2, c2, B0, c0);
+        if (k >= k1) break;
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B2, B0, c0, B1, c1);
+        if (k >= k1) break;
+    }
+}
+
+// TMA-staged slot rows (as k_step_staged) + the fan-rotation row; 1D grid with the
+// sample chunk fastest, so the chunks of one node block share its slot rows in L2.
+template <typename T, int V, bool DIFF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long nb = blockIdx.x / A.nch;
+    const int chunk = (int)(blockIdx.x - nb * A.nch);
+    const long long a0 = nb * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots) {
+        if (threadIdx.x == 0 && A.status) atomicOr(A.status, 2);
+        return;
+    }
+    const uint32_t bar = smem_u32(smem);
+    int4* srec = reinterpret_cast<int4*>(smem + 16);
+    T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_rec = (uint32_t)nsl * 16u;
+        const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        if (nsl > 0) {
+            bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+            bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+        }
+    }
+    const long long a = a0 + warp;
+    const bool active = warp < A.npb && a < a1;
+    const size_t S = (size_t)A.S;
+    const size_t col = ((size_t)chunk * 32 + lane) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    const bool clamped = a < A.n_clamped;
+    Vec<T, V> ua[3];
+    T f[3];
+    if (active && !clamped) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ua[d] = ldg<T, V>(A.u + row + d * S);
+            prefetch_l2(A.up + row + d * S);
+        }
+        prefetch_l2(A.invm + (size_t)a * S + col);
+        node_load<T>(A, a, step_pressure<T>(A), f);
+    }
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        if (lane == 0 && A.status) atomicOr(A.status, 1);
+        return;
+    }
+    if (!active) return;
+    if (clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    Vec<T, V> acc[3];
+    const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+    ku_row_fan<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+}
+
+// ------------------------------------------------------------ pipelined persistent step
+// Persistent kernel: every warp owns a private STAGES-deep ring of shared-memory
+// stages and walks its own sequence of work items (node, 32*VEC-sample chunk;
+// chunk fastest; item g = warp id + i * total warps).  For the item STAGES-1
+// ahead, each lane issues one TMA bulk copy of one row (its node's u, u_prev and
+// inverse-mass rows, every element's second-neighbour rows and coefficient row,
+// the slot records and the stiffness rows) into the stage, all completing on the
+// stage's mbarrier; meanwhile the warp multiplies the current item entirely out
+// of shared memory.  Slot records of the item after that are already in lane
+// registers, fetched one iteration earlier.  Warps never wait for each other.
+//
+// Stage layout: [0, RB*rows) rows of 32*VEC samples, then records, then stiffness
+// rows.  Rows: 0-2 u_a, 3-5 u_prev, 6 inverse mass, 7-9 first neighbour of slot 0
+// (open fans only), then 4 per slot: second neighbour (3 dofs) and coefficient.
+constexpr int kPipeFixedRows = 10;
+
+template <typename T>
+struct PipeArgs {
+    StepArgs<T> s;
+    long long n_items;
+    int stage_bytes;
+    int rec_off;   // byte offset of the records inside a stage
+    int slab_off;  // byte offset of the stiffness rows inside a stage
+    int hdr_off;   // byte offset of the header (degree, unit load) inside a stage
+    int max_deg;
+};
+
+__device__ __forceinline__ void fence_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ int4 shfl4(int4 v, int src) {
+    return make_int4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                     __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
+template <typename T, int V, bool DIFF, int STAGES>
+__global__ void __launch_bounds__(256, 1) k_step_pipe(PipeArgs<T> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const StepArgs<T>& A = P.s;
+    constexpr int LB = V * (int)sizeof(T);  // one lane's slice of a row
+    constexpr int RB = 32 * LB;             // one row of 32*VEC samples
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    unsigned char* wbase = smem + (size_t)warp * (STAGES * (size_t)P.stage_bytes + 64);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + STAGES * (size_t)P.stage_bytes);
+    if (lane < STAGES) mbar_init(smem_u32(bars + lane), 1);
+    __syncwarp();
+    const long long gw = (long long)blockIdx.x * nwarps + warp;
+    const long long GW = (long long)gridDim.x * nwarps;
+    const size_t S = (size_t)A.S;
+    const int nch = A.nch;
+
+    // Issue the stage of item g with its records in lane registers (lane k = slot k).
+    auto issue = [&](int st, long long g, int4 rq, int k0, int deg) {
+        unsigned char* sb = wbase + (size_t)st * P.stage_bytes;
+        const uint32_t bar = smem_u32(bars + st);
+        const long long a = g / nch;
+        const int chunk = (int)(g - a * nch);
+        const size_t col = (size_t)chunk * 32 * V;
+        const bool clamped = a < A.n_clamped;
+        const int4 rlast = shfl4(rq, deg > 0 ? deg - 1 : 0);
+        const int4 rfirst = shfl4(rq, 0);
+        const bool open = deg > 0 && rlast.z != rfirst.y;
+        // records and stiffness rows: two TMA bulk copies on the stage's mbarrier
+        const uint32_t b_rec = clamped ? 0u : (uint32_t)deg * 16u;
+        const uint32_t b_slab =
+            clamped ? 0u : (uint32_t)deg * (uint32_t)(kSlabStride * sizeof(T));
+        if (lane == 0) {
+            mbar_arrive_expect_tx(bar, b_rec + b_slab);
+            if (b_rec) {
+                bulk_g2s(smem_u32(sb + P.rec_off), A.rec + k0, b_rec, bar);
+                bulk_g2s(smem_u32(sb + P.slab_off), A.slab + (size_t)k0 * kSlabStride, b_slab,
+                         bar);
+            }
+        }
+        if (clamped) return;
+        // header: degree (plain store) and the node's unit load (cp.async)
+        if (lane == 0) *reinterpret_cast<int*>(sb + P.hdr_off) = deg;
+        if (lane * 16 < 4 * (int)sizeof(T))
+            cp_async<16>(smem_u32(sb + P.hdr_off + 16) + lane * 16,
+                         reinterpret_cast<const unsigned char*>(A.fhat + 4 * a) + lane * 16);
+        // rows: every lane copies its own VEC-sample slice of each row with cp.async
+        const uint32_t ls = smem_u32(sb) + lane * LB;
+        const size_t cl = col + (size_t)lane * V;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            cp_async<LB>(ls + d * RB, A.u + ((size_t)a * 3 + d) * S + cl);
+            cp_async<LB>(ls + (3 + d) * RB, A.up + ((size_t)a * 3 + d) * S + cl);
+        }
+        cp_async<LB>(ls + 6 * RB, A.invm + (size_t)a * S + cl);
+        if (open) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                cp_async<LB>(ls + (7 + d) * RB, A.u + ((size_t)rfirst.y * 3 + d) * S + cl);
+        }
+        for (int k = 0; k < deg; ++k) {
+            const int4 rs = shfl4(rq, k);
+            const uint32_t d0 = ls + (kPipeFixedRows + 4 * k) * RB;
+            const T* p2 = A.u + (size_t)rs.z * 3 * S + cl;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) cp_async<LB>(d0 + d * RB, p2 + d * S);
+            cp_async<LB>(d0 + 3 * RB, A.coef + (size_t)rs.x * S + cl);
+        }
+    };
+    // Records and slot range of item g, lane k holding slot k (deg <= 32).
+    auto fetch = [&](long long g, int4& rq, int& k0, int& deg) {
+        rq = make_int4(0, 0, 0, 0);
+        k0 = 0;
+        deg = 0;
+        if (g >= P.n_items) return;
+        const long long a = g / nch;
+        k0 = __ldg(A.node_ptr + a);
+        deg = __ldg(A.node_ptr + a + 1) - k0;
+        if (lane < deg) rq = __ldg(A.rec + k0 + lane);
+    };
+
+    const T p = step_pressure<T>(A);
+    uint32_t parity = 0;  // bit st: parity of the next completion of stage st
+    int4 rq;
+    int k0q, degq;
+    // prologue: fill STAGES-1 stages; one cp.async group per stage, empty ones included,
+    // so that "STAGES-1 groups still pending" always means the oldest one is complete
+    long long gi = gw;
+    fetch(gi, rq, k0q, degq);
+    for (int s = 0; s < STAGES - 1; ++s) {
+        const long long g = gw + s * GW;
+        if (g < P.n_items) issue(s, g, rq, k0q, degq);
+        cp_async_commit();
+        fetch(g + GW, rq, k0q, degq);
+    }
+    int st = 0;
+    for (long long g = gw; g < P.n_items; g += GW) {
+        // issue the item STAGES-1 ahead into the stage freed last iteration
+        const long long gn = g + (long long)(STAGES - 1) * GW;
+        const int stn = (st + STAGES - 1) % STAGES;
+        if (gn < P.n_items) {
+            fence_async_shared();
+            issue(stn, gn, rq, k0q, degq);
+        }
+        cp_async_commit();
+        fetch(gn + GW, rq, k0q, degq);
+        // wait for the current stage: this lane's rows, then the bulk-copied rows; the
+        // header's unit load was copied by lanes 0-1, so the warp syncs before reading it
+        cp_async_wait_group<STAGES - 1>();
+        __syncwarp();
+        const uint32_t bar = smem_u32(bars + st);
+        if (!mbar_wait_bounded(bar, (parity >> st) & 1u, kMaxPolls)) {
+            if (lane == 0 && A.status) atomicOr(A.status, 1);
+            cp_async_wait_all();
+            return;
+        }
+        parity ^= 1u << st;
+        const unsigned char* sb = wbase + (size_t)st * P.stage_bytes;
+        const long long a = g / nch;
+        const int chunk = (int)(g - a * nch);
+        const size_t col = ((size_t)chunk * 32 + lane) * V;
+        const size_t row = (size_t)a * 3 * S + col;
+        if (a < A.n_clamped) {
+            const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        } else {
+            const unsigned char* ln = sb + lane * V * sizeof(T);
+            const int4* srec = reinterpret_cast<const int4*>(sb + P.rec_off);
+            const T* sslab = reinterpret_cast<const T*>(sb + P.slab_off);
+            const int deg = *reinterpret_cast<const int*>(sb + P.hdr_off);
+            const T* fhs = reinterpret_cast<const T*>(sb + P.hdr_off + 16);
+            Vec<T, V> ua[3], acc[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ua[d] = lds<T, V>(ln + d * RB);
+                acc[d] = vzero<T, V>();
+            }
+            if (deg > 0) {
+                const bool open = srec[deg - 1].z != srec[0].y;
+                Vec<T, V> d1[3];
+                const unsigned char* x1p = open ? ln + 7 * RB : ln + (kPipeFixedRows + 4 * (deg - 1)) * RB;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) d1[d] = lds<T, V>(x1p + d * RB);
+                to_diff<T, V, DIFF>(d1, ua);
+                for (int k = 0; k < deg; ++k) {
+                    const unsigned char* xp = ln + (kPipeFixedRows + 4 * k) * RB;
+                    if (k > 0 && !(srec[k].w & 1)) {  // fan break: first neighbour from global
+                        load_rows<T, V>(d1, A.u, srec[k].y, S, col);
+                        to_diff<T, V, DIFF>(d1, ua);
+                    }
+                    Vec<T, V> d2[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) d2[d] = lds<T, V>(xp + d * RB);
+                    to_diff<T, V, DIFF>(d2, ua);
+                    const Vec<T, V> c = lds<T, V>(xp + 3 * RB);
+                    slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * k, c, d1, d2, ua, acc);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) d1[d] = d2[d];
+                }
+            }
+            // epilogue out of the stage
+            const Vec<T, V> im = lds<T, V>(ln + 6 * RB);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const Vec<T, V> up = lds<T, V>(ln + (3 + d) * RB);
+                T load = p * fhs[d];
+                if (A.trac) load += __ldg(A.trac + 4 * a + d);
+                Vec<T, V> o;
+#pragma unroll
+                for (int i = 0; i < V; ++i) {
+                    const T dv = ua[d].v[i] - up.v[i];
+                    const T w = A.w0 * im.v[i];
+                    const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+                    o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+                }
+                stcs<T, V>(A.un + row + d * S, o);
+            }
+        }
+        __syncwarp();  // every lane is done reading this stage before it is refilled
+        st = (st + 1) % STAGES;
+    }
+    // drain: no copies are left in flight (every issued stage was waited on above)
+}
+
+// ------------------------------------------------------------ cp.async gather step
+// Same block shape and TMA-staged slot rows as k_step_staged, but each warp then
+// issues the whole gather of its node at once: every lane copies its V-sample
+// slice of each needed row (first fan neighbour, each element's second neighbour
+// and coefficient, the node's u_prev rows and inverse mass) global -> shared with
+// cp.async, waits once, and multiplies entirely out of shared memory.  Data in
+// flight costs no registers, so all of a node's loads overlap.  Each lane reads
+// back only the bytes it copied itself, so no warp barrier is needed.
+
+// rows of the per-warp buffer: 3 (first x1) + 4 per slot (x2 dofs, coef) + 4 (u_prev, invm)
+__host__ __device__ constexpr int gather_rows(int max_degree) { return 7 + 4 * max_degree; }
+
+template <typename T, int V, bool DIFF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_gather(StepArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int LB = V * (int)sizeof(T);  // bytes of one lane's slice of a row
+    constexpr int RB = 32 * LB;             // bytes of one warp row
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long a0 = (long long)blockIdx.x * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots) {
+        if (threadIdx.x == 0 && A.status) atomicOr(A.status, 2);
+        return;
+    }
+    const uint32_t bar = smem_u32(smem);
+    int4* srec = reinterpret_cast<int4*>(smem + 16);
+    T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    unsigned char* wbuf = smem + 16 + (size_t)A.cap_slots * (16 + kSlabStride * sizeof(T)) +
+                          (size_t)warp * A.gather_rows * RB + lane * LB;
+    const uint32_t wsm = smem_u32(wbuf);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_rec = (uint32_t)nsl * 16u;
+        const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        if (nsl > 0) {
+            bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+            bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+        }
+    }
+    const long long a = a0 + warp;
+    const bool active = warp < A.npb && a < a1;
+    const size_t S = (size_t)A.S;
+    const size_t col = ((size_t)blockIdx.y * 32 + lane) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    const bool clamped = a < A.n_clamped;
+    Vec<T, V> ua[3];
+    int k0 = 0, k1 = 0;
+    if (active && !clamped) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
+        k0 = __ldg(A.node_ptr + a) - kb;
+        k1 = __ldg(A.node_ptr + a + 1) - kb;
+        // epilogue rows go first: they do not depend on the staged slot records
+        const int eb = 3 + 4 * (k1 - k0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) cp_async<LB>(wsm + (eb + d) * RB, A.up + row + d * S);
+        cp_async<LB>(wsm + (eb + 3) * RB, A.invm + (size_t)a * S + col);
+    }
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        if (lane == 0 && A.status) atomicOr(A.status, 1);
+        cp_async_wait_all();
+        return;
+    }
+    if (!active) return;
+    if (clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    // issue the whole gather
+    if (k1 > k0) {
+        const int4 r0 = srec[k0];
+        const T* p1 = A.u + (size_t)r0.y * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) cp_async<LB>(wsm + d * RB, p1 + d * S);
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int4 r = srec[k];
+        const uint32_t base = wsm + (3 + 4 * (k - k0)) * RB;
+        const T* p2 = A.u + (size_t)r.z * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) cp_async<LB>(base + d * RB, p2 + d * S);
+        cp_async<LB>(base + 3 * RB, A.coef + (size_t)r.x * S + col);
+    }
+    cp_async_wait_all();
+
+    Vec<T, V> acc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    for (int k = k0; k < k1; ++k) {
+        const int4 r = srec[k];
+        const unsigned char* x2p = wbuf + (3 + 4 * (k - k0)) * RB;
+        Vec<T, V> d1[3], d2[3];
+        if (k == k0 || (r.w & 1)) {
+            const unsigned char* x1p = (k == k0) ? wbuf : x2p - 4 * RB;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) d1[d] = lds<T, V>(x1p + d * RB);
+        } else {  // fan break inside the row: fetch the first neighbour directly
+            const T* p1 = A.u + (size_t)r.y * 3 * S + col;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) d1[d] = ldg<T, V>(p1 + d * S);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            d2[d] = lds<T, V>(x2p + d * RB);
+            if constexpr (DIFF) {
+                d1[d] = vsub(d1[d], ua[d]);
+                d2[d] = vsub(d2[d], ua[d]);
+            }
+        }
+        const Vec<T, V> c = lds<T, V>(x2p + 3 * RB);
+        const T* K = sslab + (size_t)kSlabStride * k;
+        T kk[28];
+        if constexpr (sizeof(T) == 4) {
+#pragma unroll
+            for (int q = (DIFF ? 2 : 0); q < 7; ++q) {
+                const float4 t = reinterpret_cast<const float4*>(K)[q];
+                kk[4 * q] = t.x;
+                kk[4 * q + 1] = t.y;
+                kk[4 * q + 2] = t.z;
+                kk[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = (DIFF ? 4 : 0); q < 14; ++q) {
+                const double2 t = reinterpret_cast<const double2*>(K)[q];
+                kk[2 * q] = t.x;
+                kk[2 * q + 1] = t.y;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            Vec<T, V> t = vzero<T, V>();
+            if constexpr (!DIFF) {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], d1[jj]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], d2[jj]);
+            vfma(acc[i], c, t);
+        }
+    }
+    // epilogue out of shared memory
+    const int eb = 3 + 4 * (k1 - k0);
+    const double pd = A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure;
+    const T p = (T)pd;
+    const Vec<T, V> im = lds<T, V>(wbuf + (eb + 3) * RB);
+    const T* fh = A.fhat + 4 * a;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const Vec<T, V> up = lds<T, V>(wbuf + (eb + d) * RB);
+        T load = p * __ldg(fh + d);
+        if (A.trac) load += __ldg(A.trac + 4 * a + d);
+        Vec<T, V> o;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const T dv = ua[d].v[i] - up.v[i];
+            const T w = A.w0 * im.v[i];
+            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+        }
+        stcs<T, V>(A.un + row + d * S, o);
+    }
+}
 
 // ------------------------------------------------------------------ norms
 constexpr int kNormThreads = 128;
@@ -534,9 +1123,10 @@ struct StepTuning {
     int staged;
     int minb;  // minimum resident blocks per SM asked of the compiler (register cap)
 };
-// Defaults from a sweep on the 256x1024 tube with 512 samples (B200).
-static StepTuning g_tune32 = {4, 4, 1, 2};
-static StepTuning g_tune64 = {2, 4, 1, 2};
+// Defaults from sweeps on the 256x1024 tube with 512 samples (B200): the fan-rotation
+// kernel, 2 nodes per block, 2 blocks per SM worth of registers.
+static StepTuning g_tune32 = {4, 2, 3, 2};
+static StepTuning g_tune64 = {2, 2, 3, 2};
 template <typename T>
 StepTuning& tuning_of() {
     return sizeof(T) == 4 ? g_tune32 : g_tune64;
@@ -556,9 +1146,76 @@ int launch_staged(K kernel, dim3 grid, int threads, size_t smem, cudaStream_t st
     return CVFES_OK;
 }
 
+inline int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+    return n > 0 ? n : 148;
+}
+
+// Persistent pipelined step: `warps` warps per block, `stages` stages per warp.
+template <typename T, int V, bool DIFF, int STAGES>
+int launch_pipe_s(const StepArgs<T>& A, long long max_deg, int warps, cudaStream_t st) {
+    constexpr int RB = 32 * V * (int)sizeof(T);
+    PipeArgs<T> P;
+    P.s = A;
+    P.n_items = A.n_nodes * A.nch;
+    P.max_deg = (int)max_deg;
+    P.rec_off = (kPipeFixedRows + 4 * (int)max_deg) * RB;
+    P.slab_off = P.rec_off + (int)max_deg * 16;
+    P.hdr_off = ((P.slab_off + (int)max_deg * kSlabStride * (int)sizeof(T)) + 15) / 16 * 16;
+    P.stage_bytes = (P.hdr_off + 64 + 127) / 128 * 128;
+    const size_t smem = (size_t)warps * ((size_t)STAGES * P.stage_bytes + 64);
+    if (smem > 227 * 1024) return CVFES_ERR_UNSUPPORTED;
+    auto kernel = k_step_pipe<T, V, DIFF, STAGES>;
+    if (smem > 48 * 1024) {
+        cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return fail(CVFES_ERR_CUDA, "k_step_pipe smem attribute: %s", cudaGetErrorString(e));
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * warps, smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        return fail(CVFES_ERR_CUDA, "k_step_pipe does not fit on an SM (%zu B smem)", smem);
+    long long blocks = (long long)per_sm * sm_count();
+    const long long need = (P.n_items + warps - 1) / warps;
+    if (blocks > need) blocks = need;
+    kernel<<<(unsigned)blocks, 32 * warps, smem, st>>>(P);
+    CVFES_LAUNCH_CHECK("k_step_pipe");
+    return CVFES_OK;
+}
+
 template <typename T, int V, bool DIFF>
-int launch_staged_v(int minb, dim3 grid, int threads, size_t smem, cudaStream_t st,
+int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, cudaStream_t st) {
+    switch (stages) {
+        case 4: return launch_pipe_s<T, V, DIFF, 4>(A, max_deg, warps, st);
+        case 3: return launch_pipe_s<T, V, DIFF, 3>(A, max_deg, warps, st);
+        default: return launch_pipe_s<T, V, DIFF, 2>(A, max_deg, warps, st);
+    }
+}
+
+template <typename T, int V, bool DIFF>
+int launch_staged_v(int variant, int minb, dim3 grid, int threads, size_t smem, cudaStream_t st,
                     const StepArgs<T>& A) {
+    if (variant == 3) {
+        const dim3 g1((unsigned)((long long)grid.x * grid.y));
+        switch (minb) {
+            case 4: return launch_staged(k_step_fan<T, V, DIFF, 4>, g1, threads, smem, st, A);
+            case 3: return launch_staged(k_step_fan<T, V, DIFF, 3>, g1, threads, smem, st, A);
+            case 2: return launch_staged(k_step_fan<T, V, DIFF, 2>, g1, threads, smem, st, A);
+            default: return launch_staged(k_step_fan<T, V, DIFF, 1>, g1, threads, smem, st, A);
+        }
+    }
+    if (variant == 2) {
+        switch (minb) {
+            case 4: return launch_staged(k_step_gather<T, V, DIFF, 4>, grid, threads, smem, st, A);
+            case 3: return launch_staged(k_step_gather<T, V, DIFF, 3>, grid, threads, smem, st, A);
+            case 2: return launch_staged(k_step_gather<T, V, DIFF, 2>, grid, threads, smem, st, A);
+            default: return launch_staged(k_step_gather<T, V, DIFF, 1>, grid, threads, smem, st, A);
+        }
+    }
     switch (minb) {
         case 4: return launch_staged(k_step_staged<T, V, DIFF, 4>, grid, threads, smem, st, A);
         case 3: return launch_staged(k_step_staged<T, V, DIFF, 3>, grid, threads, smem, st, A);
@@ -605,22 +1262,45 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     int V = pick_vec<T>(ptrs, 5, A.S);
     while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
-    // TMA-staged kernel: a warp per node needs S/V to be a multiple of 32.
+    // Pipelined persistent kernel (npb = warps per block, minb = stages per warp).
+    if (tune.staged == 4 && m->max_degree > 0 && m->max_degree <= 32 && (A.S / V) % 32 == 0) {
+        A.nch = A.S / V / 32;
+        A.npb = tune.npb;
+        A.tpn = 32;
+        A.cap_slots = 0;
+        A.gather_rows = 0;
+        const int stages = tune.minb < 2 ? 2 : (tune.minb > 4 ? 4 : tune.minb);
+        int prc = CVFES_ERR_UNSUPPORTED;
+        if (V == 4) {
+            if constexpr (sizeof(T) == 4)
+                prc = launch_pipe<T, 4, DIFF>(A, m->max_degree, tune.npb, stages, st);
+        } else if (V == 2) {
+            prc = launch_pipe<T, 2, DIFF>(A, m->max_degree, tune.npb, stages, st);
+        } else {
+            prc = launch_pipe<T, 1, DIFF>(A, m->max_degree, tune.npb, stages, st);
+        }
+        if (prc != CVFES_ERR_UNSUPPORTED) return prc;  // else fall through to a smaller kernel
+    }
+    // TMA-staged kernels: a warp per node needs S/V to be a multiple of 32.
     const long long cap = (long long)tune.npb * m->max_degree;
-    const size_t smem = 16 + (size_t)cap * (16 + kSlabStride * sizeof(T));
+    A.gather_rows = gather_rows((int)m->max_degree);
+    size_t smem = 16 + (size_t)cap * (16 + kSlabStride * sizeof(T));
+    if (tune.staged == 2) smem += (size_t)tune.npb * A.gather_rows * 32 * V * sizeof(T);
     if (tune.staged && m->max_degree > 0 && (A.S / V) % 32 == 0 && smem <= kMaxStageBytes) {
         A.npb = tune.npb;
         A.tpn = 32;
         A.cap_slots = (int)cap;
+        A.nch = A.S / V / 32;
         const dim3 grid((unsigned)((m->n_nodes + A.npb - 1) / A.npb), (unsigned)(A.S / V / 32));
         const int threads = 32 * A.npb;
         if (V == 4) {
             if constexpr (sizeof(T) == 4)
-                rc = launch_staged_v<T, 4, DIFF>(tune.minb, grid, threads, smem, st, A);
+                rc = launch_staged_v<T, 4, DIFF>(tune.staged, tune.minb, grid, threads, smem, st,
+                                                 A);
         } else if (V == 2) {
-            rc = launch_staged_v<T, 2, DIFF>(tune.minb, grid, threads, smem, st, A);
+            rc = launch_staged_v<T, 2, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A);
         } else {
-            rc = launch_staged_v<T, 1, DIFF>(tune.minb, grid, threads, smem, st, A);
+            rc = launch_staged_v<T, 1, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A);
         }
         return rc;
     }
@@ -922,7 +1602,9 @@ extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb
     StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
     t.vec = vec;
     t.npb = npb;
-    t.staged = staged ? 1 : 0;
+    if (staged < 0 || staged > 4)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..4");
+    t.staged = staged;
     t.minb = minb;
     return CVFES_OK;
 }

@@ -64,8 +64,16 @@ typedef struct cvfes_solid_mesh {
  * FP64 vec 2, 8 nodes per block, TMA-staged slot rows).
  *   precision 32 | 64;  vec: samples per thread (FP32 1|2|4, FP64 1|2);
  *   npb: nodes per block when a warp owns one node (1..8, one warp each);
- *   staged: 1 = slot records and stiffness rows staged in shared memory by a
- *           TMA bulk copy, 0 = read through L1;
+ *   staged: 0 = slot records, stiffness rows and gathers read through L1;
+ *           1 = slot records and stiffness rows staged in shared memory by a
+ *               TMA bulk copy, gathers through registers (2 elements in flight);
+ *           2 = as 1, and each warp copies its node's whole gather into shared
+ *               memory with cp.async before multiplying;
+ *           3 = as 1, with the fan's shared neighbour carried between elements
+ *               (three-buffer rotation) and the sample chunk fastest in the grid;
+ *           4 = persistent pipelined kernel: each warp streams its own work
+ *               items through a ring of `minb` (2..4) shared-memory stages
+ *               filled by per-row TMA bulk copies; npb = warps per block;
  *   minb: resident blocks per SM the register allocation must allow (1..4).
  * Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,

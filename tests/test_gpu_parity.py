@@ -204,3 +204,51 @@ def test_invalid_arguments_are_rejected(lib, cuda):
         call("cvfes_solid_step_f64", _lib.C.byref(s._desc), ptr(s.plan.coef64),
              ptr(s.plan.invm64), ptr(s.bufs[0]), ptr(s.bufs[1]), ptr(s.bufs[2]), None, None, 0,
              0.0, None, -1.0, 0.0, None)
+
+
+VARIANTS = {32: [(0, 4, 8, 1), (1, 4, 4, 2), (2, 4, 4, 2), (3, 4, 2, 2), (4, 4, 4, 2), (4, 4, 4, 3),
+                 (4, 2, 8, 3), (3, 2, 4, 3), (1, 1, 8, 4)],
+            64: [(0, 2, 8, 1), (1, 2, 4, 2), (3, 2, 2, 2), (4, 2, 4, 2), (4, 1, 6, 3), (3, 1, 4, 3)]}
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_step_kernel_variants_are_bitwise_identical(lib, cuda, precision):
+    """Every step-kernel variant (L1 gather, TMA-staged, cp.async gather, fan rotation,
+    pipelined persistent) computes the same floating-point operations in the same
+    order: their states after 60 steps must be bitwise equal."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    S = 128 if precision == 32 else 64
+    mesh = c0_mesh(S)
+    saved = _lib.get_step_tuning(precision)
+    outs = []
+    try:
+        for staged, vec, npb, minb in VARIANTS[precision]:
+            _lib.set_step_tuning(precision, vec, npb, staged, minb)
+            s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+            s.Advance(case.pressures(60))
+            s.plan.check_status()
+            outs.append(((staged, vec, npb, minb), s.local_displacement().clone()))
+            s.release_graphs()
+    finally:
+        _lib.set_step_tuning(precision, **saved)
+    ref_cfg, ref = outs[0]
+    assert torch.isfinite(ref).all()
+    for cfg, out in outs[1:]:
+        assert torch.equal(out, ref), f"variant {cfg} differs from {ref_cfg}"
+
+
+def test_large_sample_chunk_against_oracle(lib, cuda):
+    """S = 128 (the warp-per-node kernels) on the 64x128 tube, 40 steps, vs the FP64 oracle."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(128)
+    coefK, gthick = mesh.element_coefficients()
+    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
+                             mesh.density, mesh.v, mesh.damp, case.dt, backend="template")
+    pres = case.pressures(40)
+    o.run(pres)
+    for precision, tol in ((64, FP64_TOL), (32, FP32_TOL)):
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 128, precision, chunk=12))
+        s.Advance(pres)
+        assert so.rel_l2(s.displacement(), o.u) < tol
