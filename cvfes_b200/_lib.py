@@ -77,6 +77,7 @@ SIGNATURES = {
     "cvfes_norms_work_size": (C.c_int64, [I64, I64]),
     "cvfes_solid_norms_f64": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
     "cvfes_solid_norms_f32": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
+    "cvfes_solid_norms_noalloc_f32": (C.c_int, [I64, I64, P, P, P, P, I32, P]),
     "cvfes_graph_capture_advance": (C.c_int, [DESC, I32, P, P, P, P, P, P, P, I64, D, D, P,
                                               C.POINTER(C.c_void_p)]),
     "cvfes_graph_launch": (C.c_int, [P, P]),

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -1630,5 +1631,81 @@ extern "C" int cvfes_status_read(int32_t* status, void* stream) {
     CVFES_CUDA_TRY(cudaStreamSynchronize(st));
     if (h & 1) return fail(CVFES_ERR_TIMEOUT, "a bounded device wait gave up (status %d)", h);
     if (h) return fail(CVFES_ERR_ARG, "device status %d: slot stage overflow", h);
+    return CVFES_OK;
+}
+
+// ------------------------------------------------------------ allocation-free norms
+// Some callers cannot hand the library a device workspace and must not make it
+// allocate one: a watchdog that runs between the steps of a large ensemble whose
+// state fills the GPU (a cudaMalloc there can fail, and it synchronises the
+// device), or a host framework whose own memory pool owns all device memory.
+// For them the FP64 norms reduction keeps its block partials in this fixed
+// array instead of a caller workspace.  It is 4 MiB on every GPU that loads the
+// library, held until the process exits.
+constexpr long long kNormScratchDoubles = 1LL << 19;
+static __device__ __align__(256) double g_norm_scratch[kNormScratchDoubles];
+
+namespace {
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_norm_scratch_mu;
+double* g_norm_scratch_dev[kMaxScratchDevices] = {};
+}  // namespace
+
+// Device address of g_norm_scratch on the current device.  In host code the name
+// g_norm_scratch is only a host-side stand-in, so its address must come from
+// cudaGetSymbolAddress, once per device, with that device current.
+static int norm_scratch_address(double** out) {
+    int dev = -1;
+    CVFES_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxScratchDevices)
+        return fail(CVFES_ERR_UNSUPPORTED, "cvfes_solid_norms_noalloc_f32: device %d", dev);
+    std::lock_guard<std::mutex> lock(g_norm_scratch_mu);
+    if (!g_norm_scratch_dev[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(CVFES_ERR_CUDA, "cudaGetSymbolAddress(g_norm_scratch) on device %d: %s",
+                        dev, cudaGetErrorString(e));
+        g_norm_scratch_dev[dev] = static_cast<double*>(p);
+    }
+    *out = g_norm_scratch_dev[dev];
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                                             const float* u_prev, const float* invm,
+                                             double* out, int32_t check_finite, void* stream) {
+    if (n_nodes <= 0 || n_samples <= 0 || !u || !u_prev || !invm || !out)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_norms_noalloc_f32: bad argument");
+    if (4 * n_samples + 1 > kNormScratchDoubles)
+        return fail(CVFES_ERR_ARG,
+                    "cvfes_solid_norms_noalloc_f32: %lld samples exceed the fixed scratch "
+                    "(at most %lld samples)",
+                    (long long)n_samples, (kNormScratchDoubles - 1) / 4);
+    double* work = nullptr;
+    int rc = norm_scratch_address(&work);
+    if (rc) return rc;
+    const long long S = n_samples;
+    long long nch = norm_chunks(n_nodes);
+    const long long fit = (kNormScratchDoubles - 1) / (4 * S);
+    if (nch > fit) nch = fit;
+    const long long npc = (n_nodes + nch - 1) / nch;
+    nch = (n_nodes + npc - 1) / npc;
+    cudaStream_t st = (cudaStream_t)stream;
+    double* total = work + (size_t)nch * S * 4;  // the non-finite counter starts at zero
+    CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
+    dim3 grid((unsigned)nch, (unsigned)((S + kNormThreads - 1) / kNormThreads));
+    k_norms_partial<float><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, u_prev, invm,
+                                                          work);
+    CVFES_LAUNCH_CHECK("k_norms_partial (fixed scratch)");
+    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
+    CVFES_LAUNCH_CHECK("k_norms_final (fixed scratch)");
+    if (check_finite) {
+        double h = 0.0;
+        CVFES_CUDA_TRY(cudaMemcpyAsync(&h, total, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CVFES_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h != 0.0)
+            return fail(CVFES_ERR_NONFINITE, "watchdog: %.0f non-finite state values", h);
+    }
     return CVFES_OK;
 }

@@ -236,6 +236,20 @@ int cvfes_solid_norms_f32(int64_t n_nodes, int64_t n_samples, const float* u,
                           const float* u_prev, const float* invm, double* work,
                           double* out, int32_t check_finite, void* stream);
 
+/* The FP32-state norms of cvfes_solid_norms_f32 without a workspace argument and
+ * without allocating anything; no counterpart in the reference.  For callers that
+ * hold no device workspace and must not allocate one while the ensemble runs (a
+ * between-steps watchdog on a GPU whose memory the state fills, or a framework
+ * whose own pool owns all device memory).  The block partials live in a fixed
+ * 4 MiB device array compiled into the library (held on every GPU that loads it
+ * until exit), so n_samples may be at most 131071; larger requests fail with
+ * CVFES_ERR_ARG.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (e.g. on two streams) race.         */
+int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                                  const float* u_prev, const float* invm, double* out,
+                                  int32_t check_finite, void* stream);
+
 /* ------------------------------------------------------------ CUDA graphs
  * Capture `chunk` steps of cvfes_solid_advance (chunk a multiple of 3 so the
  * buffer roles repeat) plus the clock increment into one executable graph.
