@@ -322,6 +322,82 @@ def run_gpu(args):
     return 0
 
 
+def run_batched(args):
+    """64 uneven tubes (own resolution, radius, length, sample count and CFL time step)
+    advanced by one persistent launch per step; metric summed over all tubes."""
+    import torch
+    import torch.distributed as dist
+    from cvfes_b200.batched import BatchedSolidSolver
+    from cvfes_b200.cases import P_MAX, RAMP_STEPS, batched_cases, build_meshes, case_dt
+    from cvfes_b200.tune import tune_batch
+
+    rank, world, local = dist_setup(args)
+    cases = batched_cases(64, seed=7 + 1000 * rank)
+    meshes = build_meshes(cases)  # spawn pool, before any CUDA work of this process
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    prec = 32 if args.precision == "fp32" else 64
+    dts = [case_dt(c, m) for c, m in zip(cases, meshes)]
+    batch = BatchedSolidSolver(meshes, dts, precision=prec, device=dev, graph_chunk=args.chunk)
+    tuned = tune_batch(batch)
+    K, W = args.steps, args.warmup
+    pres = P_MAX * np.minimum(np.arange(W + K, dtype=np.float64) / RAMP_STEPS, 1.0)
+    stream = torch.cuda.current_stream(dev)
+    batch.Advance(pres[:W])
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local).start()
+    time.sleep(0.6)
+    t0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    batch.Advance(pres[W:W + K])
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    finite = all(bool(np.all(n[:, 3] == 0)) for n in batch.Norms(check_finite=False))
+    S_total = batch.sample_count()
+    bstep = batch.algorithmic_bytes()
+    peaks, peak_kind = measured_peaks()
+    achieved = bstep / (ms / K * 1e-3) / 1e9
+    # one step kernel per step, one clock kernel per graph chunk and per plain remainder
+    launches = K + K // batch.graph_chunk + 1
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * S_total * K / (ms_max * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == 32 else "f64", "data": "synthetic",
+            "config": {"workload": "batched64", "tubes": len(cases),
+                       "nodes": sum(m.nNodes for m in meshes),
+                       "elements": sum(m.nElements for m in meshes), "samples": S_total,
+                       "parallelism": f"replicas{world}", "tuning": tuned.get("vec"),
+                       "grid": tuned.get("grid"), "l2": "state > L2, no flush",
+                       "finite": finite},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peak_kind, "bytes_per_step": bstep},
+            "clocks": clocks.summary(t0, t1),
+        }
+        print(json.dumps(line), flush=True)
+    batch.release_graphs()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,6 +418,8 @@ def main():
         raise SystemExit("--chunk must be a multiple of 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched64":
+        return run_batched(args)
     return run_gpu(args)
 
 

@@ -48,6 +48,18 @@ class SolidMeshDesc(C.Structure):
     ]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [
+        ("mesh", SolidMeshDesc),
+        ("coef", C.c_void_p),
+        ("invm", C.c_void_p),
+        ("buf", C.c_void_p * 3),
+        ("p_sched", C.c_void_p),
+        ("dt", C.c_double),
+        ("damp", C.c_double),
+    ]
+
+
 P = C.c_void_p
 I64 = C.c_int64
 I32 = C.c_int32
@@ -85,6 +97,13 @@ SIGNATURES = {
     "cvfes_set_step_tuning": (C.c_int, [I32, I32, I32, I32, I32]),
     "cvfes_get_step_tuning": (C.c_int, [I32, P, P, P, P]),
     "cvfes_status_read": (C.c_int, [P, P]),
+    "cvfes_batch_table_bytes": (C.c_int64, [I32]),
+    "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, C.POINTER(C.c_int64)]),
+    "cvfes_batch_step": (C.c_int, [P, I32, I64, I32, I32, I32, P, I64, I32, P]),
+    "cvfes_batch_advance": (C.c_int, [P, I32, I64, I32, I32, I32, P, I64, I32,
+                                      C.POINTER(C.c_int32), P]),
+    "cvfes_batch_graph_capture": (C.c_int, [P, I32, I64, I32, I32, P, I64, I32,
+                                            C.POINTER(C.c_void_p)]),
 }
 
 

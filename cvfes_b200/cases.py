@@ -118,6 +118,44 @@ def case_dt(case: TubeCase, mesh: SolidMesh) -> float:
     return cfl_dt(mesh.nodes, mesh.elementNodeIds, float(np.max(mesh.elmE)), case.density)
 
 
+def _build_material(args):
+    """Worker of :func:`build_meshes`: the GMRF material of one case (cached on disk)."""
+    import dataclasses
+    case_dict, threads = args
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    m = build_mesh(TubeCase(**case_dict))
+    return m.elmE, m.elmThick
+
+
+def build_meshes(cases, processes: Optional[int] = None):
+    """Build many tube meshes, generating their GMRF material in parallel processes.
+
+    The pool uses the ``spawn`` start method, so it is safe to call after CUDA has
+    been initialised in the parent process.
+    """
+    import dataclasses
+    import multiprocessing as mp
+    n = len(cases)
+    cores = os.cpu_count() or 1
+    procs = max(1, min(n, processes or min(16, cores)))
+    threads = max(1, cores // procs)
+    todo = [(dataclasses.asdict(c), threads) for c in cases]
+    if procs == 1:
+        mats = [_build_material(t) for t in todo]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            mats = pool.map(_build_material, todo, chunksize=1)
+    out = []
+    for case, (elmE, elmH) in zip(cases, mats):
+        nodes, elems, inlet, outlet = tube_mesh(case.geometry())
+        out.append(SolidMesh(nodes=nodes, elementNodeIds=elems,
+                             boundary=np.concatenate([inlet, outlet]), nSmp=case.n_samples,
+                             density=case.density, v=case.nu, damp=case.damp, bdyU=0.0,
+                             elmE=elmE, elmThick=elmH, name=case.name,
+                             mass_lumping=case.mass_lumping))
+    return out
+
+
 def batched_cases(n_tubes: int = 64, seed: int = 7):
     """The 64-tube uneven ensemble: random radius, length, resolution and sample count."""
     rng = np.random.default_rng(seed)

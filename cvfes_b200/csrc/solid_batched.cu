@@ -1,0 +1,271 @@
+// Batched multi-mesh solid step: many independent tube meshes with their own node
+// counts, sample counts, time steps and pressure schedules advance together in one
+// persistent launch per step.
+//
+// The caller packs one descriptor per mesh into a device table (cvfes_batch_pack).
+// Work item w of the batch is (mesh m, node block, sample chunk) with the chunk
+// fastest; item offsets per mesh are prefix sums, so a block finds its mesh by a
+// binary search.  Blocks loop over items with a grid stride (persistent), and each
+// thread runs the same row gather K_s u_s and fused damped update as the
+// single-mesh L1 kernel, so a mesh advanced in a batch is bitwise identical to the
+// same mesh advanced alone.  All meshes rotate their three state buffers in lock
+// step; the rotation index and the step's offset into the pressure schedules are
+// launch arguments (a device clock supplies the base offset inside CUDA graphs).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "step_core.cuh"
+
+namespace cvfes {
+
+// One mesh of the batch as the kernels see it (type-agnostic pointers).
+struct BatchMesh {
+    const int32_t* node_ptr;
+    const int4* rec;
+    const void* slab;
+    const void* fhat;
+    const void* coef;
+    const void* invm;
+    void* buf[3];
+    const double* p_sched;
+    long long n_nodes;
+    long long item_off;  // first work item of this mesh
+    int S;
+    int n_clamped;
+    double clamp;
+    double eta;
+    double w0;
+    int tpn;     // threads per node chunk
+    int npb;     // nodes per block
+    int chunks;  // sample chunks per node block
+    int pad;
+};
+
+template <typename T, int V, bool DIFF>
+__global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restrict__ tab,
+                                                     int n_meshes, long long total, int rot,
+                                                     const long long* clock, long long j) {
+    const int cur = (3 - rot) % 3, prev = (cur + 1) % 3, nxt = (cur + 2) % 3;
+    const long long base = clock ? clock[0] : 0LL;
+    for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+        // mesh of item w: largest m with item_off <= w
+        int lo = 0, hi = n_meshes - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&tab[mid].item_off) <= w) lo = mid; else hi = mid - 1;
+        }
+        const BatchMesh& M = tab[lo];
+        const long long local = w - M.item_off;
+        const long long nb = local / M.chunks;
+        const int chunk = (int)(local - nb * M.chunks);
+        const int t = threadIdx.x / M.tpn;
+        if (t >= M.npb) continue;
+        const long long a = nb * M.npb + t;
+        if (a >= M.n_nodes) continue;
+        const int vec = chunk * M.tpn + (threadIdx.x - t * M.tpn);
+        StepArgs<T> A;
+        A.node_ptr = M.node_ptr;
+        A.rec = M.rec;
+        A.slab = static_cast<const T*>(M.slab);
+        A.fhat = static_cast<const T*>(M.fhat);
+        A.coef = static_cast<const T*>(M.coef);
+        A.invm = static_cast<const T*>(M.invm);
+        A.u = static_cast<const T*>(M.buf[cur]);
+        A.up = static_cast<const T*>(M.buf[prev]);
+        A.un = static_cast<T*>(M.buf[nxt]);
+        A.trac = nullptr;
+        A.p_sched = M.p_sched;
+        A.clock = nullptr;
+        A.j = base + j;
+        A.pressure = 0.0;
+        A.n_nodes = M.n_nodes;
+        A.S = M.S;
+        A.n_clamped = M.n_clamped;
+        A.clamp = (T)M.clamp;
+        A.eta = (T)M.eta;
+        A.w0 = (T)M.w0;
+        const size_t S = (size_t)M.S;
+        const size_t col = (size_t)vec * V;
+        const size_t row = (size_t)a * 3 * S + col;
+        if (a < M.n_clamped) {
+            const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+            continue;
+        }
+        Vec<T, V> ua[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ua[d] = ldg<T, V>(A.u + row + d * S);
+        T f[3];
+        node_load<T>(A, a, step_pressure<T>(A), f);
+        Vec<T, V> acc[3];
+        ku_row<T, V, DIFF>(A.node_ptr, A.rec, A.slab, A.coef, A.u, S, col, a, ua, acc);
+        step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+    }
+}
+
+__global__ void k_batch_clock_add(long long* clock, long long n) { clock[0] += n; }
+
+template <typename T>
+int launch_batched(const BatchMesh* tab, int n_meshes, long long total, int vec, int rot,
+                   const long long* clock, long long j, int grid, cudaStream_t st) {
+    constexpr bool DIFF = std::is_same<T, float>::value;
+    if (total <= 0) return CVFES_OK;
+    if (grid <= 0 || grid > total) grid = (int)(total < (1LL << 30) ? total : (1 << 30));
+    if (vec == 4) {
+        if constexpr (sizeof(T) == 4)
+            k_step_batched<T, 4, DIFF><<<grid, 256, 0, st>>>(tab, n_meshes, total, rot, clock, j);
+    } else if (vec == 2) {
+        k_step_batched<T, 2, DIFF><<<grid, 256, 0, st>>>(tab, n_meshes, total, rot, clock, j);
+    } else {
+        k_step_batched<T, 1, DIFF><<<grid, 256, 0, st>>>(tab, n_meshes, total, rot, clock, j);
+    }
+    CVFES_LAUNCH_CHECK("k_step_batched");
+    return CVFES_OK;
+}
+
+}  // namespace cvfes
+
+using namespace cvfes;
+
+extern "C" int64_t cvfes_batch_table_bytes(int32_t n_meshes) {
+    return n_meshes > 0 ? (int64_t)n_meshes * (int64_t)sizeof(BatchMesh) : 0;
+}
+
+extern "C" int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes,
+                                int32_t precision, int32_t vec, void* table_dev,
+                                int64_t* total_items) {
+    if (!items || n_meshes <= 0 || !table_dev || !total_items)
+        return fail(CVFES_ERR_ARG, "cvfes_batch_pack: bad argument");
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_batch_pack: precision must be 32 or 64");
+    const int maxv = precision == 32 ? 4 : 2;
+    if (vec < 1 || vec > maxv || (vec & (vec - 1)))
+        return fail(CVFES_ERR_ARG, "cvfes_batch_pack: vec %d not allowed", vec);
+    const size_t tsz = precision == 32 ? 4 : 8;
+    std::vector<BatchMesh> h(n_meshes);
+    long long off = 0;
+    for (int m = 0; m < n_meshes; ++m) {
+        const cvfes_batch_item& it = items[m];
+        const cvfes_solid_mesh& ms = it.mesh;
+        if (ms.n_nodes <= 0 || ms.n_samples <= 0 || ms.n_samples > INT32_MAX || !ms.node_ptr ||
+            !ms.slot_rec || !ms.slot_k || !ms.fhat || !it.coef || !it.invm || !it.buf[0] ||
+            !it.buf[1] || !it.buf[2])
+            return fail(CVFES_ERR_ARG, "cvfes_batch_pack: incomplete mesh %d", m);
+        if (ms.n_clamped < 0 || ms.n_clamped > ms.n_nodes)
+            return fail(CVFES_ERR_ARG, "cvfes_batch_pack: mesh %d clamped rows", m);
+        if (ms.n_samples % vec)
+            return fail(CVFES_ERR_ARG,
+                        "cvfes_batch_pack: mesh %d has %lld samples, not a multiple of vec %d", m,
+                        (long long)ms.n_samples, vec);
+        if (!(it.dt > 0.0)) return fail(CVFES_ERR_ARG, "cvfes_batch_pack: mesh %d dt <= 0", m);
+        const void* ptrs[5] = {it.coef, it.invm, it.buf[0], it.buf[1], it.buf[2]};
+        for (int q = 0; q < 5; ++q)
+            if (reinterpret_cast<uintptr_t>(ptrs[q]) % (vec * tsz))
+                return fail(CVFES_ERR_ARG, "cvfes_batch_pack: mesh %d buffer %d misaligned", m,
+                            q);
+        BatchMesh& b = h[m];
+        b.node_ptr = ms.node_ptr;
+        b.rec = reinterpret_cast<const int4*>(ms.slot_rec);
+        b.slab = ms.slot_k;
+        b.fhat = ms.fhat;
+        b.coef = it.coef;
+        b.invm = it.invm;
+        for (int q = 0; q < 3; ++q) b.buf[q] = it.buf[q];
+        b.p_sched = it.p_sched;
+        b.n_nodes = ms.n_nodes;
+        b.S = (int)ms.n_samples;
+        b.n_clamped = (int)ms.n_clamped;
+        b.clamp = ms.clamp_value;
+        const double g = 0.5 * it.dt * it.damp;
+        b.eta = it.dt * it.damp / (1.0 + g);
+        b.w0 = it.dt * it.dt / (1.0 + g);
+        const int sv = (int)(ms.n_samples / vec);
+        b.tpn = sv < 32 ? sv : 32;
+        b.npb = 256 / b.tpn;
+        b.chunks = sv / b.tpn;
+        b.pad = 0;
+        b.item_off = off;
+        off += ((ms.n_nodes + b.npb - 1) / b.npb) * b.chunks;
+    }
+    *total_items = off;
+    CVFES_CUDA_TRY(cudaMemcpy(table_dev, h.data(), h.size() * sizeof(BatchMesh),
+                              cudaMemcpyHostToDevice));
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_batch_step(const void* table_dev, int32_t n_meshes, int64_t total_items,
+                                int32_t precision, int32_t vec, int32_t rot,
+                                const int64_t* clock, int64_t j, int32_t grid, void* stream) {
+    if (!table_dev || n_meshes <= 0 || total_items < 0 || rot < 0 || rot > 2 ||
+        (precision != 32 && precision != 64) || (vec != 1 && vec != 2 && vec != 4) ||
+        (precision == 64 && vec == 4))
+        return fail(CVFES_ERR_ARG, "cvfes_batch_step: bad argument");
+    const auto* tab = static_cast<const BatchMesh*>(table_dev);
+    const auto* clk = reinterpret_cast<const long long*>(clock);
+    if (precision == 32)
+        return launch_batched<float>(tab, n_meshes, total_items, vec, rot, clk, j, grid,
+                                     (cudaStream_t)stream);
+    return launch_batched<double>(tab, n_meshes, total_items, vec, rot, clk, j, grid,
+                                  (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_batch_advance(const void* table_dev, int32_t n_meshes, int64_t total_items,
+                                   int32_t precision, int32_t vec, int32_t rot0, int64_t* clock,
+                                   int64_t n_steps, int32_t grid, int32_t* rot_out,
+                                   void* stream) {
+    if (n_steps < 0 || rot0 < 0 || rot0 > 2)
+        return fail(CVFES_ERR_ARG, "cvfes_batch_advance: bad argument");
+    int rot = rot0;
+    for (long long k = 0; k < n_steps; ++k) {
+        int rc = cvfes_batch_step(table_dev, n_meshes, total_items, precision, vec, rot, clock, k,
+                                  grid, stream);
+        if (rc) return rc;
+        rot = (rot + 1) % 3;
+    }
+    if (clock && n_steps > 0) {
+        k_batch_clock_add<<<1, 1, 0, (cudaStream_t)stream>>>(reinterpret_cast<long long*>(clock),
+                                                             n_steps);
+        CVFES_LAUNCH_CHECK("k_batch_clock_add");
+    }
+    if (rot_out) *rot_out = rot;
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes,
+                                         int64_t total_items, int32_t precision, int32_t vec,
+                                         int64_t* clock, int64_t chunk, int32_t grid,
+                                         cvfes_graph** out) {
+    if (!out || chunk <= 0 || chunk % 3 || !clock)
+        return fail(CVFES_ERR_ARG,
+                    "cvfes_batch_graph_capture: chunk must be a positive multiple of 3 and a "
+                    "clock is required");
+    cudaStream_t cs;
+    CVFES_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return fail(CVFES_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    }
+    int rot_end = 0;
+    const int rc = cvfes_batch_advance(table_dev, n_meshes, total_items, precision, vec, 0, clock,
+                                       chunk, grid, &rot_end, cs);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CVFES_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(CVFES_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = new cvfes_graph{graph, exec};
+    return CVFES_OK;
+}

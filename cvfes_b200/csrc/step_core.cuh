@@ -1,0 +1,234 @@
+// Device building blocks of the membrane solid step shared by the single-mesh
+// kernels (solid_step.cu) and the batched multi-mesh kernel (solid_batched.cu):
+// launch arguments, TMA / mbarrier helpers with bounded waits, the thread ->
+// (node, samples) map, the row gather K_s u_s and the fused damped update.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace cvfes {
+
+template <typename T>
+struct StepArgs {
+    const int32_t* node_ptr;
+    const int4* rec;
+    const T* slab;
+    const T* fhat;
+    const T* coef;
+    const T* invm;
+    const T* u;
+    const T* up;
+    T* un;
+    const T* trac;
+    const double* p_sched;
+    const long long* clock;
+    long long j;
+    double pressure;
+    long long n_nodes;
+    int S;
+    int n_clamped;
+    T clamp;
+    T eta;
+    T w0;
+    int tpn;
+    int npb;
+    int cap_slots;   // slot capacity of the shared-memory stage (staged kernel)
+    int gather_rows; // rows of each warp's gather buffer (gather kernel)
+    int nch;         // sample chunks per node block (staged kernels; 1D grid, chunk fastest)
+    int* status;     // bit 0: a bounded wait gave up
+};
+
+// ------------------------------------------------------------ TMA / mbarrier helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+// One-dimensional TMA bulk copy global -> this CTA's shared memory (no multicast).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.b32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after max_polls try_wait rounds (each round suspends the
+// thread for a bounded, hardware-chosen time), so a lost transfer cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase, int max_polls) {
+    for (int i = 0; i < max_polls; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+constexpr int kMaxPolls = 1 << 22;
+
+// Thread -> (node, sample vector).  A block holds `npb` consecutive nodes and
+// `tpn` consecutive sample vectors of each (tpn = min(S/VEC, 32)); blockIdx.y
+// picks the sample chunk.  The warps of one block therefore gather overlapping
+// neighbour rows and element coefficients of one sample chunk.
+__device__ __forceinline__ bool map_row(int tpn, int npb, long long n_nodes, long long& a,
+                                        int& vec) {
+    const int t = threadIdx.x / tpn;
+    if (t >= npb) return false;
+    a = (long long)blockIdx.x * npb + t;
+    vec = blockIdx.y * tpn + (threadIdx.x - t * tpn);
+    return a < n_nodes;
+}
+
+struct RowGrid {
+    dim3 grid;
+    int tpn, npb;
+};
+
+inline RowGrid row_grid(long long n_nodes, int sv, int block) {
+    RowGrid g;
+    g.tpn = sv < 32 ? sv : 32;
+    g.npb = block / g.tpn;
+    g.grid = dim3((unsigned)((n_nodes + g.npb - 1) / g.npb), (unsigned)(sv / g.tpn));
+    return g;
+}
+
+// Row a of K_s u_s for VEC samples starting at column col.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row(const int32_t* __restrict__ node_ptr,
+                                       const int4* __restrict__ rec, const T* __restrict__ slab,
+                                       const T* __restrict__ coef, const T* __restrict__ u,
+                                       size_t S, size_t col, long long a, const Vec<T, V> (&ua)[3],
+                                       Vec<T, V> (&acc)[3]) {
+    const int k0 = __ldg(node_ptr + a), k1 = __ldg(node_ptr + a + 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    Vec<T, V> carry[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) carry[d] = vzero<T, V>();
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k) {
+        const int4 r = __ldg(rec + k);
+        Vec<T, V> x1[3], x2[3];
+        if (r.w & 1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x1[d] = carry[d];
+        } else {
+            const T* p1 = u + (size_t)r.y * 3 * S + col;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x1[d] = ldg<T, V>(p1 + d * S);
+                if constexpr (DIFF) x1[d] = vsub(x1[d], ua[d]);
+            }
+        }
+        const T* p2 = u + (size_t)r.z * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x2[d] = ldg<T, V>(p2 + d * S);
+            if constexpr (DIFF) x2[d] = vsub(x2[d], ua[d]);
+        }
+        const Vec<T, V> c = ldg<T, V>(coef + (size_t)r.x * S + col);
+        const T* K = slab + (size_t)kSlabStride * k;
+        T kk[27];
+        if constexpr (std::is_same<T, float>::value) {
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const float4 t = __ldg(reinterpret_cast<const float4*>(K) + q);
+                if (4 * q + 0 < 27) kk[4 * q + 0] = t.x;
+                if (4 * q + 1 < 27) kk[4 * q + 1] = t.y;
+                if (4 * q + 2 < 27) kk[4 * q + 2] = t.z;
+                if (4 * q + 3 < 27) kk[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 14; ++q) {
+                const double2 t = __ldg(reinterpret_cast<const double2*>(K) + q);
+                if (2 * q + 0 < 27) kk[2 * q + 0] = t.x;
+                if (2 * q + 1 < 27) kk[2 * q + 1] = t.y;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            Vec<T, V> t = vzero<T, V>();
+            if constexpr (!DIFF) {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], x1[jj]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], x2[jj]);
+            vfma(acc[i], c, t);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) carry[d] = x2[d];
+    }
+}
+
+// The step's pressure: one value per launch, so it is read once at kernel entry
+// (a schedule entry indexed by the device clock, or the value passed by the host).
+template <typename T>
+__device__ __forceinline__ T step_pressure(const StepArgs<T>& A) {
+    return (T)(A.p_sched ? A.p_sched[(A.clock ? A.clock[0] : 0LL) + A.j] : A.pressure);
+}
+
+// Nodal external load p*fhat (+ traction) of node a, read early by the caller.
+template <typename T>
+__device__ __forceinline__ void node_load(const StepArgs<T>& A, long long a, T p, T (&f)[3]) {
+    const float4* q = nullptr;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) f[d] = p * __ldg(A.fhat + 4 * a + d);
+    if (A.trac) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) f[d] += __ldg(A.trac + 4 * a + d);
+    }
+    (void)q;
+}
+
+// Fused update of one node row (increment form, see the file header) and its store.
+template <typename T, int V>
+__device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
+                                              size_t col, size_t row, const Vec<T, V> (&ua)[3],
+                                              const Vec<T, V> (&acc)[3], const T (&f)[3]) {
+    const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const Vec<T, V> up = ldcs<T, V>(A.up + row + d * S);
+        const T load = f[d];
+        Vec<T, V> o;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const T dv = ua[d].v[i] - up.v[i];
+            const T w = A.w0 * im.v[i];
+            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+        }
+        stcs<T, V>(A.un + row + d * S, o);
+    }
+}
+
+}  // namespace cvfes
+
+// Executable CUDA graph handed out through the C ABI (cvfes_graph_* entry points).
+struct cvfes_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};

@@ -1,0 +1,151 @@
+"""Autotuner for the step kernels: measure candidate tile shapes, keep the fastest.
+
+Single mesh: the kernel variant, samples per thread (VEC), nodes per block and
+the register bound (``cvfes_set_step_tuning``).  Batch: samples per thread (the
+tile's sample width, 32*VEC per warp) and the persistent grid size.  Every
+candidate runs a few CUDA-graph chunks from the same saved state, timed with CUDA
+events; the state is restored afterwards, so tuning does not advance the
+simulation.  Results are cached in a JSON file keyed by the GPU name and the
+problem's shape, so later runs of the same shape skip the measurement.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from typing import Iterable, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+
+STEP_CANDIDATES = {
+    32: [(3, 4, 2, 2), (3, 4, 4, 2), (3, 4, 2, 1), (1, 4, 4, 2), (3, 2, 2, 3), (0, 4, 8, 1)],
+    64: [(3, 2, 2, 2), (3, 2, 4, 2), (1, 2, 4, 2), (3, 1, 4, 3), (0, 2, 8, 1)],
+}
+
+
+def _cache_path() -> str:
+    d = os.environ.get("CVFES_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "cvfes_b200"))
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, "tuning.json")
+
+
+def _load_cache() -> dict:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(key: str, value) -> None:
+    c = _load_cache()
+    c[key] = value
+    tmp = _cache_path() + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(c, f, indent=1)
+    os.replace(tmp, _cache_path())
+
+
+def _key(kind: str, device, shape) -> str:
+    name = torch.cuda.get_device_name(device)
+    h = hashlib.sha1(repr(shape).encode()).hexdigest()[:16]
+    return f"{kind}|{name}|{h}"
+
+
+def _time_ms(fn, device) -> float:
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize(device)
+    return e0.elapsed_time(e1)
+
+
+def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] = None,
+              steps: int = 96, use_cache: bool = True) -> dict:
+    """Pick (variant, vec, npb, minb) for ``solver``'s precision and problem shape."""
+    prec = solver.precision
+    dev = solver.device
+    shape = ("step", prec, solver.lclNNodes, solver.nElms, solver.nSmp, solver.plan.max_degree)
+    key = _key("step", dev, shape)
+    cache = _load_cache() if use_cache else {}
+    if key in cache:
+        best = cache[key]
+        _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
+        return dict(best, cached=True)
+    saved = [b.clone() for b in solver.bufs]
+    roles = (solver.cur, solver.prev, solver.nxt)
+    pres = np.zeros(steps + solver.graph_chunk)
+    results = []
+    for staged, vec, npb, minb in (candidates or STEP_CANDIDATES[prec]):
+        try:
+            _lib.set_step_tuning(prec, vec, npb, staged, minb)
+        except _lib.CvfesError:
+            continue
+        solver.release_graphs()
+        for b, s in zip(solver.bufs, saved):
+            b.copy_(s)
+        solver.cur, solver.prev, solver.nxt = roles
+        solver.Advance(pres[:solver.graph_chunk])  # capture + warm
+        ms = _time_ms(lambda: solver.Advance(pres[:steps]), dev) / steps
+        results.append((ms, dict(staged=staged, vec=vec, npb=npb, minb=minb, ms_per_step=ms)))
+    for b, s in zip(solver.bufs, saved):
+        b.copy_(s)
+    solver.cur, solver.prev, solver.nxt = roles
+    solver.release_graphs()
+    best = min(results, key=lambda r: r[0])[1]
+    _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
+    if use_cache:
+        _store(key, best)
+    return dict(best, cached=False, tried=[r[1] for r in results])
+
+
+def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
+               grids: Optional[Sequence[int]] = None, steps: int = 48,
+               use_cache: bool = True) -> dict:
+    """Pick the batch's samples per thread and persistent grid size."""
+    dev = batch.device
+    shape = ("batch", batch.precision, tuple((s.lclNNodes, s.nElms, s.nSmp) for s in batch.solvers))
+    key = _key("batch", dev, shape)
+    cache = _load_cache() if use_cache else {}
+    if key in cache:
+        best = cache[key]
+        batch.set_launch(vec=best["vec"], grid=best["grid"])
+        return dict(best, cached=True)
+    maxv = 4 if batch.precision == 32 else 2
+    if vecs is None:
+        vecs = [v for v in (4, 2, 1) if v <= maxv and all(s.nSmp % v == 0 for s in batch.solvers)]
+    if grids is None:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        grids = [0, 4 * sms, 8 * sms, 16 * sms]
+    saved = [[b.clone() for b in s.bufs] for s in batch.solvers]
+    rot0 = batch.rot
+    pres = np.zeros(steps + batch.graph_chunk + 2)
+    results = []
+    for vec in vecs:
+        for grid in grids:
+            batch.set_launch(vec=vec, grid=grid)
+            for s, sv in zip(batch.solvers, saved):
+                for b, x in zip(s.bufs, sv):
+                    b.copy_(x)
+            batch.rot = rot0
+            batch.Advance(pres[:batch.graph_chunk + 2])
+            ms = _time_ms(lambda: batch.Advance(pres[:steps]), dev) / steps
+            results.append((ms, dict(vec=vec, grid=grid, ms_per_step=ms)))
+    for s, sv in zip(batch.solvers, saved):
+        for b, x in zip(s.bufs, sv):
+            b.copy_(x)
+    batch.rot = rot0
+    best = min(results, key=lambda r: r[0])[1]
+    batch.set_launch(vec=best["vec"], grid=best["grid"])
+    cur = (3 - batch.rot) % 3
+    for s in batch.solvers:
+        s.cur, s.prev, s.nxt = cur, (cur + 1) % 3, (cur + 2) % 3
+    if use_cache:
+        _store(key, best)
+    return dict(best, cached=False, tried=[r[1] for r in results])

@@ -60,8 +60,8 @@ typedef struct cvfes_solid_mesh {
                                      device wait gave up (read by cvfes_status_read) */
 } cvfes_solid_mesh;
 
-/* Step-kernel tuning (the autotuner sets these; defaults are FP32 vec 4 and
- * FP64 vec 2, 8 nodes per block, TMA-staged slot rows).
+/* Step-kernel tuning (the autotuner sets these; defaults: variant 3, FP32 vec 4,
+ * FP64 vec 2, 2 nodes per block, minb 2).
  *   precision 32 | 64;  vec: samples per thread (FP32 1|2|4, FP64 1|2);
  *   npb: nodes per block when a warp owns one node (1..8, one warp each);
  *   staged: 0 = slot records, stiffness rows and gathers read through L1;
@@ -73,7 +73,7 @@ typedef struct cvfes_solid_mesh {
  *               (three-buffer rotation) and the sample chunk fastest in the grid;
  *           4 = persistent pipelined kernel: each warp streams its own work
  *               items through a ring of `minb` (2..4) shared-memory stages
- *               filled by per-row TMA bulk copies; npb = warps per block;
+ *               (rows by cp.async, slot rows by TMA); npb = warps per block;
  *   minb: resident blocks per SM the register allocation must allow (1..4).
  * Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,
@@ -262,6 +262,40 @@ int cvfes_graph_capture_advance(const cvfes_solid_mesh* mesh, int32_t precision,
                                 double dt, double damp, void* stream, cvfes_graph** out);
 int cvfes_graph_launch(cvfes_graph* g, void* stream);
 int cvfes_graph_destroy(cvfes_graph* g);
+
+/* ------------------------------------------------------------ batched meshes
+ * Many independent meshes (own node and sample counts, time step, damping,
+ * pressure schedule) advanced together, one persistent launch per step (the
+ * batched form of the per-step solid path; the reference runs one mesh per MPI
+ * rank, physicsSolverSDampGPUs.py:325-399).  The caller allocates a device table of
+ * cvfes_batch_table_bytes(n) bytes; cvfes_batch_pack fills it (synchronous copy)
+ * and returns the number of work items.  All meshes rotate their buffers in lock
+ * step: with rot = (steps taken) % 3, u_n = buf[(3-rot)%3], u_{n-1} = buf[(4-rot)%3].
+ * vec: samples per thread (FP32 1|2|4, FP64 1|2), must divide every mesh's S.
+ * grid: blocks of the persistent launch (<= 0: one block per work item).       */
+typedef struct cvfes_batch_item {
+    cvfes_solid_mesh mesh;       /* descriptor of this mesh (device arrays)     */
+    const void*      coef;       /* [E][S] T                                    */
+    const void*      invm;       /* [N][S] T                                    */
+    void*            buf[3];     /* rotating state buffers [3N][S] T            */
+    const double*    p_sched;    /* device pressure schedule or NULL (p = 0)    */
+    double           dt;         /* this mesh's time step                       */
+    double           damp;       /* mass-proportional damping                   */
+} cvfes_batch_item;
+
+int64_t cvfes_batch_table_bytes(int32_t n_meshes);
+int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes, int32_t precision,
+                     int32_t vec, void* table_dev, int64_t* total_items);
+int cvfes_batch_step(const void* table_dev, int32_t n_meshes, int64_t total_items,
+                     int32_t precision, int32_t vec, int32_t rot, const int64_t* clock,
+                     int64_t j, int32_t grid, void* stream);
+int cvfes_batch_advance(const void* table_dev, int32_t n_meshes, int64_t total_items,
+                        int32_t precision, int32_t vec, int32_t rot0, int64_t* clock,
+                        int64_t n_steps, int32_t grid, int32_t* rot_out, void* stream);
+/* `chunk` batched steps (multiple of 3) and the clock increment as one graph. */
+int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, int64_t total_items,
+                              int32_t precision, int32_t vec, int64_t* clock, int64_t chunk,
+                              int32_t grid, cvfes_graph** out);
 
 #ifdef __cplusplus
 }
