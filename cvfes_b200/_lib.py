@@ -60,6 +60,34 @@ class BatchItem(C.Structure):
     ]
 
 
+class AdjointDesc(C.Structure):
+    _fields_ = [
+        ("mesh", SolidMeshDesc),
+        ("precision", C.c_int32),
+        ("record", C.c_int32),
+        ("coef", C.c_void_p),
+        ("invm", C.c_void_p),
+        ("owner_blocks", C.c_void_p),
+        ("state", C.c_void_p * 3),
+        ("adj", C.c_void_p * 2),
+        ("ckpt", C.c_void_p),
+        ("p_sched", C.c_void_p),
+        ("clock", C.c_void_p),
+        ("n_steps", C.c_int64),
+        ("ckpt_every", C.c_int64),
+        ("n_obs", C.c_int32),
+        ("obs_every", C.c_int32),
+        ("obs_nodes", C.c_void_p),
+        ("obs", C.c_void_p),
+        ("jpart", C.c_void_p),
+        ("J", C.c_void_p),
+        ("gamma", C.c_void_p),
+        ("gmass", C.c_void_p),
+        ("dt", C.c_double),
+        ("damp", C.c_double),
+    ]
+
+
 P = C.c_void_p
 I64 = C.c_int64
 I32 = C.c_int32
@@ -104,6 +132,17 @@ SIGNATURES = {
                                       C.POINTER(C.c_int32), P]),
     "cvfes_batch_graph_capture": (C.c_int, [P, I32, I64, I32, I32, P, I64, I32,
                                             C.POINTER(C.c_void_p)]),
+    "cvfes_adjoint_ckpt_count": (C.c_int64, [I64, I64]),
+    "cvfes_adjoint_jpart_size": (C.c_int64, [I64, I32, I32, I64]),
+    "cvfes_adjoint_owner_blocks": (C.c_int, [DESC, I32, P, P, P, P]),
+    "cvfes_adjoint_material": (C.c_int, [I64, I64, P, P, P, P, P, P]),
+    "cvfes_adjoint_forward": (C.c_int, [C.POINTER(AdjointDesc), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32), P]),
+    "cvfes_adjoint_reverse": (C.c_int, [C.POINTER(AdjointDesc), I32, I32, P]),
+    "cvfes_adjoint_gradients": (C.c_int, [C.POINTER(AdjointDesc), P, P, P, P, P, P, P, P, P]),
+    "cvfes_adjoint_capture": (C.c_int, [C.POINTER(AdjointDesc), I32, I32, I32,
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_void_p)]),
 }
 
 

@@ -79,7 +79,8 @@ CASES = {
                           extra=dict(n_obs=512, obs_every=10, ckpt_every=50)),
     "stenosed512x2048": TubeCase("stenosed512x2048", 512, 2048, 5.0, stenosed=True,
                                  n_samples=128, dt=None, n_steps=1000,
-                                 extra=dict(n_obs=4096, obs_every=10, ckpt_every=100)),
+                                 extra=dict(n_obs=4096, obs_every=10, ckpt_every=100,
+                                            grad_logh=True)),
 }
 
 
@@ -168,3 +169,41 @@ def batched_cases(n_tubes: int = 64, seed: int = 7):
                             radius=float(rng.uniform(0.15, 0.6)), n_samples=S, dt=None,
                             n_steps=1000, seed_E=1000 + i, seed_h=2000 + i))
     return out
+
+
+def adjoint_setup(case: TubeCase, precision: int = 64, device="cuda", n_samples=None,
+                  n_steps=None, grad_logh=None, use_graph=True, obs_seed: int = 99,
+                  true_seed_offset: int = 500):
+    """The mismatch workload of an adjoint case.
+
+    Returns ``(problem, logE, logh, logE_true)``: the :class:`MismatchProblem` with
+    observations recorded from a forward run whose log E field comes from a GMRF of a
+    different seed (``seed_E + true_seed_offset``), and the (E, S) FP64 starting
+    material (the case's own GMRF sample) at which gradients are taken.  Observation
+    nodes are a seeded choice of distinct free nodes.
+    """
+    import dataclasses
+
+    import torch
+
+    from .adjoint import MismatchProblem
+    S = case.n_samples if n_samples is None else n_samples
+    T = case.n_steps if n_steps is None else n_steps
+    mesh = build_mesh(case, n_samples=S)
+    true = build_mesh(dataclasses.replace(case, seed_E=case.seed_E + true_seed_offset),
+                      n_samples=S)
+    dt = case_dt(case, mesh)
+    ex = case.extra
+    free = np.setdiff1d(np.arange(mesh.nNodes), mesh.boundary)
+    rng = np.random.default_rng(obs_seed)
+    obs = np.sort(rng.choice(free, size=min(int(ex.get("n_obs", 512)), len(free)), replace=False))
+    if grad_logh is None:
+        grad_logh = bool(ex.get("grad_logh", False))
+    problem = MismatchProblem(mesh, dt, case.pressures(T), obs, obs_every=int(ex.get("obs_every", 10)),
+                              ckpt_every=int(ex.get("ckpt_every", 50)), precision=precision,
+                              device=device, grad_logh=grad_logh, use_graph=use_graph)
+    logE = torch.from_numpy(np.log(mesh.elmE))
+    logh = torch.from_numpy(np.log(mesh.elmThick))
+    logE_true = torch.from_numpy(np.log(true.elmE))
+    problem.set_observations(problem.record_observations(logE_true, logh))
+    return problem, logE, logh, logE_true

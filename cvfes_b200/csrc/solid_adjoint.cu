@@ -1,0 +1,725 @@
+// Discrete adjoint of the explicit membrane time step for a displacement-mismatch
+// objective, with respect to per-element, per-sample log E and log h.
+//
+// Forward step n (n = 0 .. T-1), free rows, W = w0 * inverse lumped mass:
+//     u_{n+1} = u_n + (1 - eta)(u_n - u_{n-1}) + W (p_n fhat - K(c) u_n),   K(c) = sum_e c_e Khat_e
+// clamped rows hold the clamp value, c_e = E_e h_e, and the objective is
+//     J_s = sum_{n in O} sum_{i in obs} |u_n(i) - uobs_n(i)|^2,   O = {n : n % obs_every == 0, n > 0}.
+// With chi_n = W mu_n (mu the adjoint of u_n, zero on clamped rows) the reverse
+// recursion has the form of the forward step:
+//     chi_n = chi_{n+1} + (1 - eta)(chi_{n+1} - chi_{n+2}) - W K chi_{n+1} + W dJ/du_n
+// and the gradients are
+//     dJ/dlogE_e = -c_e Gamma_e,   Gamma_e = sum_n chi_{n+1,e}^T Khat_e u_{n,e}
+//     dJ/dlogh_e = -c_e Gamma_e - h_e sum_{a in e} alpha_{e,a} invm_a G_a,   G_a = sum_n chi_{n+1,a} . r_{n,a}
+// with r_n = p_n fhat - K u_n and alpha_{e,a} the element's lumped-mass weight of node a
+// (m_a = sum_e h_e alpha_{e,a}).  The damping is mass-proportional, so eta does not
+// depend on the material.
+//
+// States u_n are not stored: the reverse sweep runs the forward step backwards,
+//     u_{n-1} = u_n - ((u_{n+1} - u_n) - W r_n) / (1 - eta),
+// in the same kernel that advances chi, and replaces the reconstructed pair by the
+// exact pair (u_m, u_{m+1}) saved by the forward pass at every checkpoint m (every
+// ckpt_every steps), so the reconstruction drift never spans more than one segment.
+// Both recursions share one pass over the node's slots: the fan-ordered slot rows of
+// Khat are applied to u_n and chi_{n+1}, and the slot of each element's local node 0
+// (its owner) also evaluates the element's bilinear form from the difference
+// vectors (u_b - u_a, chi_b - chi_a), which needs only the blocks K_b1b1, K_b1b2,
+// K_b2b2 of that slot's two neighbours (rigid translations are in Khat's null space).
+// Every element and node accumulator is written by one thread: no atomics.
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "common.cuh"
+#include "step_core.cuh"
+
+namespace cvfes {
+
+constexpr int kObsChunk = 16;   // observation nodes per block of the mismatch kernel
+constexpr int kOwnStride = 28;  // K_b1b1 (9), K_b1b2 (9), K_b2b2 (9), pad
+
+struct MassWeights {
+    double w[9];  // w[3a + g]: lumped-mass weight of local node a at quadrature point g
+};
+
+// Owner-slot neighbour blocks of every element, in the owner slot's (b1, b2) order.
+template <typename T>
+__global__ void k_owner_blocks(long long n_elems, const int32_t* __restrict__ elems,
+                               const int32_t* __restrict__ elem_slot,
+                               const int32_t* __restrict__ slot_rec, const T* __restrict__ slab,
+                               T* __restrict__ own) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= n_elems) return;
+    const int s0 = elem_slot[3 * e];
+    const int b1 = slot_rec[4 * s0 + 1], b2 = slot_rec[4 * s0 + 2];
+    const int l1 = elems[3 * e + 1] == b1 ? 1 : 2;
+    const int s1 = elem_slot[3 * e + l1], s2 = elem_slot[3 * e + 3 - l1];
+    const int q = slot_rec[4 * s1 + 1] == b2 ? 1 : 2;  // block of b2 in b1's slot
+    T* o = own + (size_t)kOwnStride * e;
+    const T* k1 = slab + (size_t)kSlabStride * s1;
+    const T* k2 = slab + (size_t)kSlabStride * s2;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        o[i] = k1[i];
+        o[9 + i] = k1[9 * q + i];
+        o[18 + i] = k2[i];
+    }
+    o[27] = T(0);
+}
+
+// coef = E*h and thickness h from the log-material of each element and sample.
+__global__ void k_material_log(long long n, const double* __restrict__ logE,
+                               const double* __restrict__ logh, double* __restrict__ coef64,
+                               float* __restrict__ coef32, double* __restrict__ thick) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h = exp(logh[i]);
+    const double c = exp(logE[i]) * h;
+    if (coef64) coef64[i] = c;
+    if (coef32) coef32[i] = (float)c;
+    if (thick) thick[i] = h;
+}
+
+// Observation step k: either record u at the observation nodes, or add the squared
+// mismatch of this block's observation nodes into jpart[k][block][s].
+template <typename T>
+__global__ void k_obs(int n_obs, int S, const int32_t* __restrict__ obs_nodes,
+                      const T* __restrict__ u, T* __restrict__ obs_k, double* __restrict__ jpart_k,
+                      int record) {
+    const int s = blockIdx.y * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const int i0 = blockIdx.x * kObsChunk;
+    const int i1 = min(n_obs, i0 + kObsChunk);
+    double acc = 0.0;
+    for (int i = i0; i < i1; ++i) {
+        const size_t a = (size_t)obs_nodes[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T v = u[(3 * a + c) * S + s];
+            const size_t o = ((size_t)i * 3 + c) * S + s;
+            if (record) {
+                obs_k[o] = v;
+            } else {
+                const double d = (double)v - (double)obs_k[o];
+                acc = fma(d, d, acc);
+            }
+        }
+    }
+    if (!record) jpart_k[(size_t)blockIdx.x * S + s] = acc;
+}
+
+// J[s] = sum over observation steps and node blocks, in a fixed order.
+__global__ void k_obs_reduce(long long n_parts, int S, const double* __restrict__ jpart,
+                             double* __restrict__ J) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    double acc = 0.0;
+    for (long long k = 0; k < n_parts; ++k) acc += jpart[(size_t)k * S + s];
+    J[s] = acc;
+}
+
+// chi_n += W dJ/du_n = W * 2 (u_n - uobs_n) at the free observation nodes.
+template <typename T>
+__global__ void k_adj_force(int n_obs, int S, const int32_t* __restrict__ obs_nodes,
+                            int n_clamped, const T* __restrict__ invm, T w0,
+                            const T* __restrict__ u, const T* __restrict__ obs_k, T* __restrict__ chi) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long i = g / S;
+    if (i >= n_obs) return;
+    const int s = (int)(g - i * S);
+    const size_t a = (size_t)obs_nodes[i];
+    if ((long long)a < n_clamped) return;
+    const T w = w0 * invm[a * S + s];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const size_t r = (3 * a + c) * S + s;
+        const T d = u[r] - obs_k[((size_t)i * 3 + c) * S + s];
+        chi[r] += w * T(2) * d;
+    }
+}
+
+template <typename T>
+struct RevArgs {
+    const int32_t* node_ptr;
+    const int4* rec;
+    const T* slab;
+    const T* own;
+    const T* fhat;
+    const T* coef;
+    const T* invm;
+    const T* u;    // u_n
+    T* uo;         // in: u_{n+1}; out: u_{n-1}
+    const T* x;    // chi_{n+1}
+    T* xo;         // in: chi_{n+2}; out: chi_n (without the observation forcing)
+    T* gam;        // (E, S) Gamma accumulator
+    T* gm;         // (N, S) G accumulator, or null
+    const double* p;  // pressure of forward step n
+    long long n_nodes;
+    int S;
+    int n_clamped;
+    T clamp;
+    T eta;
+    T inv1meta;
+    T w0;
+    int tpn;
+    int npb;
+};
+
+template <typename T>
+__device__ __forceinline__ void load27(const T* K, T (&kk)[27]) {
+    if constexpr (std::is_same<T, float>::value) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(K) + q);
+            if (4 * q + 0 < 27) kk[4 * q + 0] = t.x;
+            if (4 * q + 1 < 27) kk[4 * q + 1] = t.y;
+            if (4 * q + 2 < 27) kk[4 * q + 2] = t.z;
+            if (4 * q + 3 < 27) kk[4 * q + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 14; ++q) {
+            const double2 t = __ldg(reinterpret_cast<const double2*>(K) + q);
+            if (2 * q + 0 < 27) kk[2 * q + 0] = t.x;
+            if (2 * q + 1 < 27) kk[2 * q + 1] = t.y;
+        }
+    }
+}
+
+// One reverse step for (node a, V samples): reconstruct u_{n-1}, advance chi, accumulate
+// Gamma over the elements this node owns and G of this node.
+template <typename T, int V, bool DIFF, bool GM>
+__global__ void __launch_bounds__(256) k_reverse(RevArgs<T> A) {
+    long long a;
+    int vec;
+    if (!map_row(A.tpn, A.npb, A.n_nodes, A.S / V, a, vec)) return;
+    const size_t S = (size_t)A.S;
+    const size_t col = (size_t)vec * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    Vec<T, V> ua[3], ca[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ua[d] = ldg<T, V>(A.u + row + d * S);
+        ca[d] = ldg<T, V>(A.x + row + d * S);
+    }
+    const T p = (T)A.p[0];
+    Vec<T, V> accU[3], accC[3], cu[3], cc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        accU[d] = vzero<T, V>();
+        accC[d] = vzero<T, V>();
+        cu[d] = vzero<T, V>();
+        cc[d] = vzero<T, V>();
+    }
+    const int k0 = __ldg(A.node_ptr + a), k1 = __ldg(A.node_ptr + a + 1);
+    for (int k = k0; k < k1; ++k) {
+        const int4 r = __ldg(A.rec + k);
+        Vec<T, V> x1[3], x2[3], y1[3], y2[3];
+        if (r.w & 1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x1[d] = cu[d];
+                y1[d] = cc[d];
+            }
+        } else {
+            const size_t o1 = (size_t)r.y * 3 * S + col;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x1[d] = ldg<T, V>(A.u + o1 + d * S);
+                y1[d] = ldg<T, V>(A.x + o1 + d * S);
+                if constexpr (DIFF) {
+                    x1[d] = vsub(x1[d], ua[d]);
+                    y1[d] = vsub(y1[d], ca[d]);
+                }
+            }
+        }
+        const size_t o2 = (size_t)r.z * 3 * S + col;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x2[d] = ldg<T, V>(A.u + o2 + d * S);
+            y2[d] = ldg<T, V>(A.x + o2 + d * S);
+            if constexpr (DIFF) {
+                x2[d] = vsub(x2[d], ua[d]);
+                y2[d] = vsub(y2[d], ca[d]);
+            }
+        }
+        const Vec<T, V> c = ldg<T, V>(A.coef + (size_t)r.x * S + col);
+        T kk[27];
+        load27<T>(A.slab + (size_t)kSlabStride * k, kk);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            Vec<T, V> tu = vzero<T, V>(), tc = vzero<T, V>();
+            if constexpr (!DIFF) {
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                    axpy(tu, kk[3 * i + jj], ua[jj]);
+                    axpy(tc, kk[3 * i + jj], ca[jj]);
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) {
+                axpy(tu, kk[9 + 3 * i + jj], x1[jj]);
+                axpy(tc, kk[9 + 3 * i + jj], y1[jj]);
+            }
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) {
+                axpy(tu, kk[18 + 3 * i + jj], x2[jj]);
+                axpy(tc, kk[18 + 3 * i + jj], y2[jj]);
+            }
+            vfma(accU[i], c, tu);
+            vfma(accC[i], c, tc);
+        }
+        if (((r.w >> 8) & 3) == 0) {
+            // owner slot: Gamma_e += dchi^T Khat du over the two neighbours
+            Vec<T, V> du1[3], du2[3], dy1[3], dy2[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if constexpr (DIFF) {
+                    du1[d] = x1[d];
+                    du2[d] = x2[d];
+                    dy1[d] = y1[d];
+                    dy2[d] = y2[d];
+                } else {
+                    du1[d] = vsub(x1[d], ua[d]);
+                    du2[d] = vsub(x2[d], ua[d]);
+                    dy1[d] = vsub(y1[d], ca[d]);
+                    dy2[d] = vsub(y2[d], ca[d]);
+                }
+            }
+            T ob[27];
+            load27<T>(A.own + (size_t)kOwnStride * r.x, ob);
+            Vec<T, V> g = vzero<T, V>();
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                Vec<T, V> z1 = vzero<T, V>(), z2 = vzero<T, V>();
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                    axpy(z1, ob[3 * i + jj], du1[jj]);        // K_b1b1
+                    axpy(z1, ob[9 + 3 * i + jj], du2[jj]);    // K_b1b2
+                    axpy(z2, ob[9 + 3 * jj + i], du1[jj]);    // K_b2b1 = K_b1b2^T
+                    axpy(z2, ob[18 + 3 * i + jj], du2[jj]);   // K_b2b2
+                }
+                vfma(g, dy1[i], z1);
+                vfma(g, dy2[i], z2);
+            }
+            T* gp = A.gam + (size_t)r.x * S + col;
+            Vec<T, V> gv = ld<T, V>(gp);
+#pragma unroll
+            for (int q = 0; q < V; ++q) gv.v[q] += g.v[q];
+            st<T, V>(gp, gv);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            cu[d] = x2[d];
+            cc[d] = y2[d];
+        }
+    }
+    if (a < A.n_clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp), z = vzero<T, V>();
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            st<T, V>(A.uo + row + d * S, cl);
+            st<T, V>(A.xo + row + d * S, z);
+        }
+        return;
+    }
+    const Vec<T, V> im = ldg<T, V>(A.invm + (size_t)a * S + col);
+    Vec<T, V> gacc = vzero<T, V>();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T f = p * __ldg(A.fhat + 4 * a + d);
+        const Vec<T, V> u1 = ld<T, V>(A.uo + row + d * S);
+        const Vec<T, V> x2o = ld<T, V>(A.xo + row + d * S);
+        Vec<T, V> um, xn;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const bool live = im.v[i] != T(0);
+            const T w = A.w0 * im.v[i];
+            const T r = f - accU[d].v[i];
+            const T dv = ((u1.v[i] - ua[d].v[i]) - w * r) * A.inv1meta;
+            um.v[i] = live ? ua[d].v[i] - dv : T(0);
+            const T dx = ca[d].v[i] - x2o.v[i];
+            xn.v[i] = live ? ca[d].v[i] + fma(-A.eta, dx, dx) - w * accC[d].v[i] : T(0);
+            if constexpr (GM) gacc.v[i] = fma(ca[d].v[i], r, gacc.v[i]);
+        }
+        st<T, V>(A.uo + row + d * S, um);
+        st<T, V>(A.xo + row + d * S, xn);
+    }
+    if constexpr (GM) {
+        T* gp = A.gm + (size_t)a * S + col;
+        Vec<T, V> gv = ld<T, V>(gp);
+#pragma unroll
+        for (int q = 0; q < V; ++q) gv.v[q] += gacc.v[q];
+        st<T, V>(gp, gv);
+    }
+}
+
+// dJ/dlogE = -c Gamma; dJ/dlogh = -c Gamma - h sum_a alpha_{e,a} G_a / m_a.
+template <typename T>
+__global__ void k_grad_final(long long n_elems, int S, const int32_t* __restrict__ elems,
+                             const double* __restrict__ area, MassWeights mw,
+                             const double* __restrict__ lm, const double* __restrict__ logE,
+                             const double* __restrict__ logh, const T* __restrict__ gam,
+                             const T* __restrict__ gm, double* __restrict__ gE,
+                             double* __restrict__ gh) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long e = g / S;
+    if (e >= n_elems) return;
+    const int s = (int)(g - e * S);
+    const size_t o = (size_t)e * S + s;
+    const double h = exp(logh[o]);
+    const double c = exp(logE[o]) * h;
+    const double ge = -c * (double)gam[o];
+    if (gE) gE[o] = ge;
+    if (gh) {
+        double m = 0.0;
+        if (gm) {
+#pragma unroll
+            for (int la = 0; la < 3; ++la) {
+                const size_t na = (size_t)elems[3 * e + la];
+                const double alpha = area[e] * (mw.w[3 * la] + mw.w[3 * la + 1] + mw.w[3 * la + 2]);
+                m += alpha * (double)gm[na * S + s] / lm[na * S + s];
+            }
+        }
+        gh[o] = ge - h * m;
+    }
+}
+
+template <typename T>
+int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T* x, T* xo,
+                        long long n, cudaStream_t st) {
+    const cvfes_solid_mesh* m = &d->mesh;
+    RevArgs<T> A;
+    A.node_ptr = m->node_ptr;
+    A.rec = reinterpret_cast<const int4*>(m->slot_rec);
+    A.slab = static_cast<const T*>(m->slot_k);
+    A.own = static_cast<const T*>(d->owner_blocks);
+    A.fhat = static_cast<const T*>(m->fhat);
+    A.coef = static_cast<const T*>(d->coef);
+    A.invm = static_cast<const T*>(d->invm);
+    A.u = u;
+    A.uo = uo;
+    A.x = x;
+    A.xo = xo;
+    A.gam = static_cast<T*>(d->gamma);
+    A.gm = static_cast<T*>(d->gmass);
+    A.p = d->p_sched + n;
+    A.n_nodes = m->n_nodes;
+    A.S = (int)m->n_samples;
+    A.n_clamped = (int)m->n_clamped;
+    A.clamp = (T)m->clamp_value;
+    const double g = 0.5 * d->dt * d->damp;
+    const double eta = d->dt * d->damp / (1.0 + g);
+    A.eta = (T)eta;
+    A.inv1meta = (T)(1.0 / (1.0 - eta));
+    A.w0 = (T)(d->dt * d->dt / (1.0 + g));
+    const void* ptrs[8] = {d->coef, d->invm, u, uo, x, xo, d->gamma, d->gmass};
+    const int maxv = (int)(16 / sizeof(T));
+    int V = maxv;
+    for (; V > 1; V /= 2) {
+        bool ok = A.S % V == 0;
+        for (int i = 0; i < 8; ++i)
+            if (ptrs[i] && reinterpret_cast<uintptr_t>(ptrs[i]) % (V * sizeof(T))) ok = false;
+        if (ok) break;
+    }
+    const int block = 256;
+    const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
+    A.tpn = rg.tpn;
+    A.npb = rg.npb;
+    constexpr bool DIFF = std::is_same<T, float>::value;
+    const bool gmv = d->gmass != nullptr;
+    if (V == 4) {
+        if constexpr (sizeof(T) == 4) {
+            if (gmv) k_reverse<T, 4, DIFF, true><<<rg.grid, block, 0, st>>>(A);
+            else k_reverse<T, 4, DIFF, false><<<rg.grid, block, 0, st>>>(A);
+        }
+    } else if (V == 2) {
+        if (gmv) k_reverse<T, 2, DIFF, true><<<rg.grid, block, 0, st>>>(A);
+        else k_reverse<T, 2, DIFF, false><<<rg.grid, block, 0, st>>>(A);
+    } else {
+        if (gmv) k_reverse<T, 1, DIFF, true><<<rg.grid, block, 0, st>>>(A);
+        else k_reverse<T, 1, DIFF, false><<<rg.grid, block, 0, st>>>(A);
+    }
+    CVFES_LAUNCH_CHECK("k_reverse");
+    return CVFES_OK;
+}
+
+int check_adjoint(const cvfes_adjoint_desc* d, const char* who) {
+    if (!d) return fail(CVFES_ERR_ARG, "%s: null descriptor", who);
+    const cvfes_solid_mesh* m = &d->mesh;
+    if (m->n_nodes <= 0 || m->n_samples <= 0 || m->n_samples > INT32_MAX || !m->node_ptr ||
+        !m->slot_rec || !m->slot_k || !m->fhat)
+        return fail(CVFES_ERR_ARG, "%s: incomplete mesh descriptor", who);
+    if (d->precision != 32 && d->precision != 64)
+        return fail(CVFES_ERR_ARG, "%s: precision must be 32 or 64", who);
+    if (d->n_steps <= 0 || d->ckpt_every <= 0 || d->obs_every <= 0 || d->n_obs < 0)
+        return fail(CVFES_ERR_ARG, "%s: steps, checkpoint and observation intervals must be "
+                    "positive", who);
+    if (!d->coef || !d->invm || !d->owner_blocks || !d->state[0] || !d->state[1] ||
+        !d->state[2] || !d->adj[0] || !d->adj[1] || !d->ckpt || !d->p_sched || !d->clock ||
+        !d->J || !d->gamma)
+        return fail(CVFES_ERR_ARG, "%s: null buffer", who);
+    if (d->n_obs > 0 && (!d->obs_nodes || !d->obs || !d->jpart))
+        return fail(CVFES_ERR_ARG, "%s: observation buffers missing", who);
+    if (!(d->dt > 0.0)) return fail(CVFES_ERR_ARG, "%s: dt must be positive", who);
+    return CVFES_OK;
+}
+
+template <typename T>
+int adjoint_forward(const cvfes_adjoint_desc* d, int* out_cur, int* out_prev, cudaStream_t st) {
+    int rc = check_adjoint(d, "cvfes_adjoint_forward");
+    if (rc) return rc;
+    const cvfes_solid_mesh* m = &d->mesh;
+    const long long S = m->n_samples, N = m->n_nodes, T_ = d->n_steps;
+    const long long C = d->ckpt_every, K = d->obs_every;
+    const size_t state = (size_t)3 * N * S;
+    const size_t sbytes = state * sizeof(T);
+    T* buf[3] = {static_cast<T*>(d->state[0]), static_cast<T*>(d->state[1]),
+                 static_cast<T*>(d->state[2])};
+    T* ck = static_cast<T*>(d->ckpt);
+    T* obs = static_cast<T*>(d->obs);
+    for (int q = 0; q < 3; ++q) CVFES_CUDA_TRY(cudaMemsetAsync(buf[q], 0, sbytes, st));
+    CVFES_CUDA_TRY(cudaMemsetAsync(d->clock, 0, sizeof(int64_t), st));
+    CVFES_CUDA_TRY(cudaMemsetAsync(d->J, 0, S * sizeof(double), st));
+    const int nchunk = (d->n_obs + kObsChunk - 1) / kObsChunk;
+    int cur = 0, prev = 1, nxt = 2;
+    long long n = 0;
+    while (n < T_) {
+        long long next = T_;
+        const long long no = (n / K + 1) * K;
+        if (no < next) next = no;
+        long long mc = (n / C) * C + 1;
+        if (mc <= n) mc += C;
+        if (mc < next) next = mc;
+        int ci = 0, pi = 1;
+        const int order[3] = {cur, prev, nxt};
+        if constexpr (sizeof(T) == 8)
+            rc = cvfes_solid_advance_f64(m, static_cast<const double*>(d->coef),
+                                         static_cast<const double*>(d->invm), buf[cur], buf[prev],
+                                         buf[nxt], d->p_sched, d->clock, next - n, d->dt, d->damp,
+                                         &ci, &pi, st);
+        else
+            rc = cvfes_solid_advance_f32(m, static_cast<const float*>(d->coef),
+                                         static_cast<const float*>(d->invm), buf[cur], buf[prev],
+                                         buf[nxt], d->p_sched, d->clock, next - n, d->dt, d->damp,
+                                         &ci, &pi, st);
+        if (rc) return rc;
+        cur = order[ci];
+        prev = order[pi];
+        nxt = 3 - cur - prev;
+        n = next;
+        if ((n - 1) % C == 0) {
+            T* slot = ck + (size_t)((n - 1) / C) * 2 * state;
+            CVFES_CUDA_TRY(cudaMemcpyAsync(slot, buf[prev], sbytes, cudaMemcpyDeviceToDevice, st));
+            CVFES_CUDA_TRY(
+                cudaMemcpyAsync(slot + state, buf[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+        }
+        if (n % K == 0 && d->n_obs > 0) {
+            const long long k = n / K - 1;
+            dim3 grid((unsigned)nchunk, (unsigned)((S + 127) / 128));
+            k_obs<T><<<grid, 128, 0, st>>>(d->n_obs, (int)S, d->obs_nodes, buf[cur],
+                                           obs + (size_t)k * d->n_obs * 3 * S,
+                                           d->jpart + (size_t)k * nchunk * S, d->record);
+            CVFES_LAUNCH_CHECK("k_obs");
+        }
+    }
+    const long long n_obs_steps = T_ / K;
+    if (!d->record && d->n_obs > 0 && n_obs_steps > 0) {
+        k_obs_reduce<<<(unsigned)((S + 127) / 128), 128, 0, st>>>(n_obs_steps * nchunk, (int)S,
+                                                                 d->jpart, d->J);
+        CVFES_LAUNCH_CHECK("k_obs_reduce");
+    }
+    if (out_cur) *out_cur = cur;
+    if (out_prev) *out_prev = prev;
+    return CVFES_OK;
+}
+
+template <typename T>
+int adjoint_force(const cvfes_adjoint_desc* d, const T* u, T* chi, long long k, cudaStream_t st) {
+    if (d->n_obs <= 0) return CVFES_OK;
+    const long long S = d->mesh.n_samples;
+    const double g = 0.5 * d->dt * d->damp;
+    const T w0 = (T)(d->dt * d->dt / (1.0 + g));
+    k_adj_force<T><<<grid_1d((long long)d->n_obs * S, 256), 256, 0, st>>>(
+        d->n_obs, (int)S, d->obs_nodes, (int)d->mesh.n_clamped, static_cast<const T*>(d->invm),
+        w0, u, static_cast<const T*>(d->obs) + (size_t)k * d->n_obs * 3 * S, chi);
+    CVFES_LAUNCH_CHECK("k_adj_force");
+    return CVFES_OK;
+}
+
+template <typename T>
+int adjoint_reverse(const cvfes_adjoint_desc* d, int cur, int prev, cudaStream_t st) {
+    int rc = check_adjoint(d, "cvfes_adjoint_reverse");
+    if (rc) return rc;
+    if (cur < 0 || cur > 2 || prev < 0 || prev > 2 || cur == prev)
+        return fail(CVFES_ERR_ARG, "cvfes_adjoint_reverse: bad final state roles");
+    const cvfes_solid_mesh* m = &d->mesh;
+    const long long S = m->n_samples, N = m->n_nodes, E = m->n_elems, T_ = d->n_steps;
+    const long long C = d->ckpt_every, K = d->obs_every;
+    const size_t state = (size_t)3 * N * S;
+    const size_t sbytes = state * sizeof(T);
+    T* uA = static_cast<T*>(d->state[prev]);  // u_n      (starts at u_{T-1})
+    T* uB = static_cast<T*>(d->state[cur]);   // u_{n+1}  (starts at u_T)
+    T* xA = static_cast<T*>(d->adj[0]);       // chi_{n+1}
+    T* xB = static_cast<T*>(d->adj[1]);       // chi_{n+2}
+    const T* ck = static_cast<const T*>(d->ckpt);
+    CVFES_CUDA_TRY(cudaMemsetAsync(xA, 0, sbytes, st));
+    CVFES_CUDA_TRY(cudaMemsetAsync(xB, 0, sbytes, st));
+    CVFES_CUDA_TRY(cudaMemsetAsync(d->gamma, 0, (size_t)E * S * sizeof(T), st));
+    if (d->gmass) CVFES_CUDA_TRY(cudaMemsetAsync(d->gmass, 0, (size_t)N * S * sizeof(T), st));
+    if (T_ % K == 0) {
+        rc = adjoint_force<T>(d, uB, xA, T_ / K - 1, st);
+        if (rc) return rc;
+    }
+    for (long long n = T_ - 1; n >= 0; --n) {
+        if (n % C == 0) {
+            const T* slot = ck + (size_t)(n / C) * 2 * state;
+            CVFES_CUDA_TRY(cudaMemcpyAsync(uA, slot, sbytes, cudaMemcpyDeviceToDevice, st));
+            CVFES_CUDA_TRY(
+                cudaMemcpyAsync(uB, slot + state, sbytes, cudaMemcpyDeviceToDevice, st));
+        }
+        rc = launch_reverse_step<T>(d, uA, uB, xA, xB, n, st);
+        if (rc) return rc;
+        T* t = uA;
+        uA = uB;
+        uB = t;
+        t = xA;
+        xA = xB;
+        xB = t;
+        // now uA = u_{n-1}, uB = u_n, xA = chi_n, xB = chi_{n+1}
+        if (n > 0 && n % K == 0) {
+            rc = adjoint_force<T>(d, uB, xA, n / K - 1, st);
+            if (rc) return rc;
+        }
+    }
+    return CVFES_OK;
+}
+
+template <typename F>
+int capture(F&& issue, cvfes_graph** out) {
+    cudaStream_t cs;
+    CVFES_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return fail(CVFES_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    }
+    const int rc = issue(cs);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CVFES_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(CVFES_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = new cvfes_graph{graph, exec};
+    return CVFES_OK;
+}
+
+}  // namespace cvfes
+
+using namespace cvfes;
+
+extern "C" int64_t cvfes_adjoint_ckpt_count(int64_t n_steps, int64_t ckpt_every) {
+    if (n_steps <= 0 || ckpt_every <= 0) return 0;
+    return (n_steps + ckpt_every - 1) / ckpt_every;
+}
+
+extern "C" int64_t cvfes_adjoint_jpart_size(int64_t n_steps, int32_t obs_every, int32_t n_obs,
+                                            int64_t n_samples) {
+    if (n_steps <= 0 || obs_every <= 0 || n_obs <= 0 || n_samples <= 0) return 0;
+    return (n_steps / obs_every) * ((n_obs + kObsChunk - 1) / kObsChunk) * n_samples;
+}
+
+extern "C" int cvfes_adjoint_owner_blocks(const cvfes_solid_mesh* mesh, int32_t precision,
+                                          const int32_t* elems, const int32_t* elem_slot,
+                                          void* out, void* stream) {
+    if (!mesh || mesh->n_elems <= 0 || !mesh->slot_rec || !mesh->slot_k || !elems || !elem_slot ||
+        !out || (precision != 32 && precision != 64))
+        return fail(CVFES_ERR_ARG, "cvfes_adjoint_owner_blocks: bad argument");
+    const long long E = mesh->n_elems;
+    if (precision == 64)
+        k_owner_blocks<double><<<grid_1d(E, 256), 256, 0, (cudaStream_t)stream>>>(
+            E, elems, elem_slot, mesh->slot_rec, static_cast<const double*>(mesh->slot_k),
+            static_cast<double*>(out));
+    else
+        k_owner_blocks<float><<<grid_1d(E, 256), 256, 0, (cudaStream_t)stream>>>(
+            E, elems, elem_slot, mesh->slot_rec, static_cast<const float*>(mesh->slot_k),
+            static_cast<float*>(out));
+    CVFES_LAUNCH_CHECK("k_owner_blocks");
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_adjoint_material(int64_t n_elems, int64_t n_samples, const double* logE,
+                                      const double* logh, double* coef64, float* coef32,
+                                      double* thick, void* stream) {
+    if (n_elems <= 0 || n_samples <= 0 || !logE || !logh || (!coef64 && !coef32 && !thick))
+        return fail(CVFES_ERR_ARG, "cvfes_adjoint_material: bad argument");
+    const long long n = n_elems * n_samples;
+    k_material_log<<<grid_1d(n, 256), 256, 0, (cudaStream_t)stream>>>(n, logE, logh, coef64,
+                                                                        coef32, thick);
+    CVFES_LAUNCH_CHECK("k_material_log");
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_adjoint_forward(const cvfes_adjoint_desc* d, int32_t* final_cur,
+                                     int32_t* final_prev, void* stream) {
+    if (!d) return fail(CVFES_ERR_ARG, "cvfes_adjoint_forward: null descriptor");
+    if (d->precision == 64) return adjoint_forward<double>(d, final_cur, final_prev, (cudaStream_t)stream);
+    return adjoint_forward<float>(d, final_cur, final_prev, (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_adjoint_reverse(const cvfes_adjoint_desc* d, int32_t final_cur,
+                                     int32_t final_prev, void* stream) {
+    if (!d) return fail(CVFES_ERR_ARG, "cvfes_adjoint_reverse: null descriptor");
+    if (d->precision == 64) return adjoint_reverse<double>(d, final_cur, final_prev, (cudaStream_t)stream);
+    return adjoint_reverse<float>(d, final_cur, final_prev, (cudaStream_t)stream);
+}
+
+extern "C" int cvfes_adjoint_gradients(const cvfes_adjoint_desc* d, const int32_t* elems,
+                                       const double* area, const double* mass_weights,
+                                       const double* lm, const double* logE, const double* logh,
+                                       double* grad_logE, double* grad_logh, void* stream) {
+    int rc = check_adjoint(d, "cvfes_adjoint_gradients");
+    if (rc) return rc;
+    if (!elems || !area || !logE || !logh || (!grad_logE && !grad_logh))
+        return fail(CVFES_ERR_ARG, "cvfes_adjoint_gradients: bad argument");
+    if (grad_logh && (!d->gmass || !lm || !mass_weights))
+        return fail(CVFES_ERR_ARG,
+                    "cvfes_adjoint_gradients: the log h gradient needs the G accumulator, the "
+                    "lumped mass and the mass weights");
+    MassWeights mw{};
+    if (mass_weights)
+        for (int i = 0; i < 9; ++i) mw.w[i] = mass_weights[i];
+    const long long E = d->mesh.n_elems, S = d->mesh.n_samples;
+    if (d->precision == 64)
+        k_grad_final<double><<<grid_1d(E * S, 256), 256, 0, (cudaStream_t)stream>>>(
+            E, (int)S, elems, area, mw, lm, logE, logh, static_cast<const double*>(d->gamma),
+            static_cast<const double*>(d->gmass), grad_logE, grad_logh);
+    else
+        k_grad_final<float><<<grid_1d(E * S, 256), 256, 0, (cudaStream_t)stream>>>(
+            E, (int)S, elems, area, mw, lm, logE, logh, static_cast<const float*>(d->gamma),
+            static_cast<const float*>(d->gmass), grad_logE, grad_logh);
+    CVFES_LAUNCH_CHECK("k_grad_final");
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_adjoint_capture(const cvfes_adjoint_desc* d, int32_t which, int32_t cur,
+                                     int32_t prev, int32_t* final_cur, int32_t* final_prev,
+                                     cvfes_graph** out) {
+    if (!d || !out || (which != 0 && which != 1))
+        return fail(CVFES_ERR_ARG, "cvfes_adjoint_capture: bad argument");
+    return capture(
+        [&](cudaStream_t cs) -> int {
+            if (which == 0) return cvfes_adjoint_forward(d, final_cur, final_prev, cs);
+            return cvfes_adjoint_reverse(d, cur, prev, cs);
+        },
+        out);
+}

@@ -39,7 +39,7 @@ struct BatchMesh {
     double w0;
     int tpn;     // threads per node chunk
     int npb;     // nodes per block
-    int chunks;  // sample chunks per node block
+    int chunks;  // sample chunks per node block (the last one may be partial)
     int pad;
 };
 
@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restric
         const long long a = nb * M.npb + t;
         if (a >= M.n_nodes) continue;
         const int vec = chunk * M.tpn + (threadIdx.x - t * M.tpn);
+        if (vec * V >= M.S) continue;  // last chunk of S/V not a multiple of 32
         StepArgs<T> A;
         A.node_ptr = M.node_ptr;
         A.rec = M.rec;
@@ -185,7 +186,7 @@ extern "C" int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes,
         const int sv = (int)(ms.n_samples / vec);
         b.tpn = sv < 32 ? sv : 32;
         b.npb = 256 / b.tpn;
-        b.chunks = sv / b.tpn;
+        b.chunks = (sv + b.tpn - 1) / b.tpn;
         b.pad = 0;
         b.item_off = off;
         off += ((ms.n_nodes + b.npb - 1) / b.npb) * b.chunks;

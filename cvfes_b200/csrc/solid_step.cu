@@ -37,7 +37,7 @@ template <typename T, int V, bool DIFF>
 __global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
     long long a;
     int vec;
-    if (!map_row(A.tpn, A.npb, A.n_nodes, a, vec)) return;
+    if (!map_row(A.tpn, A.npb, A.n_nodes, A.S / V, a, vec)) return;
     const size_t S = (size_t)A.S;
     const size_t col = (size_t)vec * V;
     const size_t row = (size_t)a * 3 * S + col;
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256)
            T* res, long long n_nodes, int S_, int accumulate, int tpn, int npb) {
     long long a;
     int vec;
-    if (!map_row(tpn, npb, n_nodes, a, vec)) return;
+    if (!map_row(tpn, npb, n_nodes, S_ / V, a, vec)) return;
     const size_t S = (size_t)S_;
     const size_t col = (size_t)vec * V;
     const size_t row = (size_t)a * 3 * S + col;

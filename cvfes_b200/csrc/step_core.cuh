@@ -87,15 +87,16 @@ constexpr int kMaxPolls = 1 << 22;
 
 // Thread -> (node, sample vector).  A block holds `npb` consecutive nodes and
 // `tpn` consecutive sample vectors of each (tpn = min(S/VEC, 32)); blockIdx.y
-// picks the sample chunk.  The warps of one block therefore gather overlapping
+// picks the sample chunk, the last one partly filled when S/VEC is not a
+// multiple of 32.  The warps of one block therefore gather overlapping
 // neighbour rows and element coefficients of one sample chunk.
-__device__ __forceinline__ bool map_row(int tpn, int npb, long long n_nodes, long long& a,
-                                        int& vec) {
+__device__ __forceinline__ bool map_row(int tpn, int npb, long long n_nodes, int sv,
+                                        long long& a, int& vec) {
     const int t = threadIdx.x / tpn;
     if (t >= npb) return false;
     a = (long long)blockIdx.x * npb + t;
     vec = blockIdx.y * tpn + (threadIdx.x - t * tpn);
-    return a < n_nodes;
+    return a < n_nodes && vec < sv;
 }
 
 struct RowGrid {
@@ -107,7 +108,7 @@ inline RowGrid row_grid(long long n_nodes, int sv, int block) {
     RowGrid g;
     g.tpn = sv < 32 ? sv : 32;
     g.npb = block / g.tpn;
-    g.grid = dim3((unsigned)((n_nodes + g.npb - 1) / g.npb), (unsigned)(sv / g.tpn));
+    g.grid = dim3((unsigned)((n_nodes + g.npb - 1) / g.npb), (unsigned)((sv + g.tpn - 1) / g.tpn));
     return g;
 }
 

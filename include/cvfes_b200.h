@@ -297,6 +297,75 @@ int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, int64_t t
                               int32_t precision, int32_t vec, int64_t* clock, int64_t chunk,
                               int32_t grid, cvfes_graph** out);
 
+/* ------------------------------------------------------------ adjoint
+ * Gradient of the displacement-mismatch objective
+ *     J_s = sum_{n % obs_every == 0, 0 < n <= T} sum_{i in obs} |u_n(i) - uobs_n(i)|^2
+ * with respect to per-element, per-sample log E and log h (inverse wall-stiffness
+ * estimation).  No counterpart in the reference, which has no differentiation.
+ * The run starts from rest (u_0 = u_{-1} = 0: zero initial displacement and
+ * velocity and zero pressure at t = 0, the reference's default start).
+ * The forward pass runs T steps, adds up J and saves the pair (u_m, u_{m+1}) at
+ * m = 0, C, 2C, ... (C = ckpt_every); the reverse pass runs the adjoint recursion
+ * and the forward step backwards from u_T, restarting from each saved pair, and
+ * accumulates Gamma (E x S) and optionally G (N x S); cvfes_adjoint_gradients turns
+ * them into dJ/dlogE and dJ/dlogh.  All buffers are device memory at the problem's
+ * precision T unless typed.                                                       */
+typedef struct cvfes_adjoint_desc {
+    cvfes_solid_mesh mesh;        /* templates and records at this precision         */
+    int32_t      precision;       /* 32 or 64                                        */
+    int32_t      record;          /* 1: the forward stores u at the observation nodes
+                                     into obs instead of adding up J                 */
+    const void*  coef;            /* [E][S] E*h                                      */
+    const void*  invm;            /* [N][S] inverse lumped mass                      */
+    const void*  owner_blocks;    /* [E][28] from cvfes_adjoint_owner_blocks         */
+    void*        state[3];        /* [3N][S] forward ring; final roles are returned  */
+    void*        adj[2];          /* [3N][S] adjoint pair                            */
+    void*        ckpt;            /* [ckpt_count][2][3N][S]                          */
+    const double* p_sched;        /* [T] pressure of forward step n                  */
+    int64_t*     clock;           /* device step counter of the forward steps        */
+    int64_t      n_steps;         /* T                                               */
+    int64_t      ckpt_every;      /* C                                               */
+    int32_t      n_obs;           /* observation nodes (0: J = 0)                    */
+    int32_t      obs_every;       /* observation interval in steps                   */
+    const int32_t* obs_nodes;     /* [n_obs] distinct node ids                       */
+    void*        obs;             /* [T/obs_every][n_obs][3][S] observed u           */
+    double*      jpart;           /* [cvfes_adjoint_jpart_size] scratch              */
+    double*      J;               /* [S] objective                                   */
+    void*        gamma;           /* [E][S] sum_n chi_{n+1}^T Khat_e u_n             */
+    void*        gmass;           /* [N][S] sum_n chi_{n+1} . (p_n fhat - K u_n), or
+                                     NULL when no log h gradient is wanted           */
+    double       dt;
+    double       damp;
+} cvfes_adjoint_desc;
+
+int64_t cvfes_adjoint_ckpt_count(int64_t n_steps, int64_t ckpt_every);
+int64_t cvfes_adjoint_jpart_size(int64_t n_steps, int32_t obs_every, int32_t n_obs,
+                                 int64_t n_samples);
+/* Per element, the blocks K_b1b1, K_b1b2, K_b2b2 of the unit stiffness in the order of
+ * the slot of its local node 0 (elems [E][3] int32, elem_slot [E][3] int32). */
+int cvfes_adjoint_owner_blocks(const cvfes_solid_mesh* mesh, int32_t precision,
+                               const int32_t* elems, const int32_t* elem_slot, void* out,
+                               void* stream);
+/* coef = exp(logE) exp(logh) (FP64 and/or FP32 copy) and thick = exp(logh), [E][S]. */
+int cvfes_adjoint_material(int64_t n_elems, int64_t n_samples, const double* logE,
+                           const double* logh, double* coef64, float* coef32, double* thick,
+                           void* stream);
+int cvfes_adjoint_forward(const cvfes_adjoint_desc* d, int32_t* final_cur, int32_t* final_prev,
+                          void* stream);
+int cvfes_adjoint_reverse(const cvfes_adjoint_desc* d, int32_t final_cur, int32_t final_prev,
+                          void* stream);
+/* grad_logE = -c Gamma; grad_logh = grad_logE - h sum_a alpha_{e,a} G_a / m_a, [E][S] FP64.
+ * mass_weights: the 9 lumped-mass weights w[3a+g] of cvfes_solid_mass_load_f64;
+ * area [E] and lm [N][S] FP64 as produced there. */
+int cvfes_adjoint_gradients(const cvfes_adjoint_desc* d, const int32_t* elems,
+                            const double* area, const double* mass_weights, const double* lm,
+                            const double* logE, const double* logh, double* grad_logE,
+                            double* grad_logh, void* stream);
+/* which = 0: the forward pass (returns the final roles); 1: the reverse pass from
+ * roles (cur, prev).  The graph replays against the descriptor's buffers. */
+int cvfes_adjoint_capture(const cvfes_adjoint_desc* d, int32_t which, int32_t cur, int32_t prev,
+                          int32_t* final_cur, int32_t* final_prev, cvfes_graph** out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -252,3 +252,26 @@ def test_large_sample_chunk_against_oracle(lib, cuda):
         s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 128, precision, chunk=12))
         s.Advance(pres)
         assert so.rel_l2(s.displacement(), o.u) < tol
+
+
+@pytest.mark.parametrize("S", [200, 72])
+def test_partial_sample_chunks_against_oracle(lib, cuda, S):
+    """S/VEC above 32 and not a multiple of 32 (last sample chunk of a node block partly
+    filled): every sample still steps, FP64 and FP32, single mesh and batch."""
+    from cvfes_b200.batched import BatchedSolidSolver
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(S)
+    coefK, gthick = mesh.element_coefficients()
+    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
+                             mesh.density, mesh.v, mesh.damp, case.dt, backend="template")
+    pres = case.pressures(30)
+    o.run(pres)
+    for precision, tol in ((64, FP64_TOL), (32, FP32_TOL)):
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+        s.Advance(pres)
+        assert so.rel_l2(s.displacement(), o.u) < tol
+        b = BatchedSolidSolver([mesh], [case.dt], precision=precision, device=cuda,
+                               graph_chunk=12)
+        b.Advance(pres)
+        assert so.rel_l2(b.displacement(0), o.u) < tol
