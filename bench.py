@@ -322,6 +322,136 @@ def run_gpu(args):
     return 0
 
 
+def adjoint_bytes(N, E, S, b, bt, log_h):
+    """Bytes one reverse step must move: per sample u_n, u_{n+1} read and u_{n-1}
+    written (backward reconstruction, 9N), chi_{n+1}, chi_{n+2} read and chi_n written
+    (9N), inverse mass (N), coefficient (E), the Gamma accumulator read and written
+    (2E) and, for log h, the G accumulator (2N); shared data as in the forward step."""
+    return S * b * (19 * N + 3 * E + (2 * N if log_h else 0)) + E * (12 + 45 * bt) + 3 * N * bt
+
+
+def run_adjoint(args):
+    """Forward + adjoint gradient evaluations of the mismatch objective; a bench step is
+    one evaluation (T forward steps, then T reverse steps and the gradient)."""
+    import torch
+    from cvfes_b200.adjoint import wall_mismatch
+    from cvfes_b200.cases import CASES, adjoint_setup
+
+    rank, world, local = dist_setup(args)
+    case = CASES[args.workload]
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
+    prec = 32 if args.precision == "fp32" else 64
+    import dataclasses
+    rcase = dataclasses.replace(case, seed_E=case.seed_E + 1000 * rank,
+                                seed_h=case.seed_h + 1000 * rank)
+    problem, logE, logh, _ = adjoint_setup(rcase, precision=prec, device=dev)
+    S, N, E, T = problem.S, problem.N, problem.E, problem.T
+    log_h = problem.grad_logh
+    logE_d, logh_d = logE.to(dev), logh.to(dev)
+    stream = torch.cuda.current_stream(dev)
+    K, W = args.steps, args.warmup
+    for _ in range(W):
+        problem.objective(logE_d, logh_d)
+        problem.gradient()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local).start()
+    time.sleep(0.6)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3 * K)]
+    t0 = time.perf_counter()
+    for k in range(K):
+        evs[3 * k].record(stream)
+        problem.objective(logE_d, logh_d)
+        evs[3 * k + 1].record(stream)
+        problem.gradient()
+        evs[3 * k + 2].record(stream)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    clocks.stop()
+    fwd = sum(evs[3 * k].elapsed_time(evs[3 * k + 1]) for k in range(K))
+    adj = sum(evs[3 * k + 1].elapsed_time(evs[3 * k + 2]) for k in range(K))
+    tot = torch.tensor([fwd + adj, fwd, adj], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    ms_tot, ms_fwd, ms_adj = (float(x) for x in tot.cpu())
+    finite = bool(torch.isfinite(problem.J).all())
+
+    # e2e through the autograd.Function with host tensors in and gradients out
+    lE_h = logE.to(torch.float64).pin_memory()
+    lh_h = logh.to(torch.float64).pin_memory()
+    gE_h = torch.empty_like(lE_h).pin_memory()
+    gh_h = torch.empty_like(lh_h).pin_memory() if log_h else None
+    J_h = torch.empty(S, dtype=torch.float64).pin_memory()
+    K2 = max(1, min(K, 2))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(K2):
+        lE = lE_h.to(dev, non_blocking=True).requires_grad_(True)
+        lh = lh_h.to(dev, non_blocking=True).requires_grad_(log_h)
+        J = wall_mismatch(lE, lh, problem)
+        J.sum().backward()
+        J_h.copy_(J.detach(), non_blocking=True)
+        gE_h.copy_(lE.grad, non_blocking=True)
+        if log_h:
+            gh_h.copy_(lh.grad, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = e0.elapsed_time(e1)
+    problem.release_graphs()
+
+    b = 4 if prec == 32 else 8
+    b_fwd = algorithmic_bytes(N, E, S, b, b)
+    b_rev = adjoint_bytes(N, E, S, b, b, log_h)
+    peaks, peak_kind = measured_peaks()
+    achieved = b_rev / (ms_adj / K / T * 1e-3) / 1e9
+    nck = (T + problem.ckpt_every - 1) // problem.ckpt_every
+    launches_fwd = T + (T // problem.obs_every) + 2 * T // 48 + 4
+    launches_rev = T + (T // problem.obs_every) + 1
+    if rank == 0:
+        line = {
+            "metric": "sample-timesteps/s (fwd+adjoint)",
+            "value": world * S * T * K / (ms_tot * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_tot / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == 32 else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "nodes": N, "elements": E, "samples": S,
+                       "time_steps": T, "dt": problem.dt, "obs_nodes": problem.n_obs,
+                       "obs_every": problem.obs_every, "ckpt_every": problem.ckpt_every,
+                       "checkpoints": nck, "params": "logE,logh" if log_h else "logE",
+                       "parallelism": f"replicas{world}", "l2": "state > L2, no flush",
+                       "finite": finite, "step": "one gradient evaluation (T forward + T "
+                                                 "reverse time steps)"},
+            "adjoint": {"fwd_ms": ms_fwd / K, "adj_ms": ms_adj / K,
+                        "ratio_fwd_plus_adj_over_fwd": ms_tot / ms_fwd,
+                        "gradients_per_s": world * S * K / (ms_tot * 1e-3),
+                        "fwd_sample_timesteps_per_s": world * S * T * K / (ms_fwd * 1e-3),
+                        "fwd_bytes_per_step": b_fwd, "rev_bytes_per_step": b_rev,
+                        "fwd_hbm_frac": b_fwd / (ms_fwd / K / T * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+            "e2e": {"value": world * S * T * K2 / (ms_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": 2 * E * S * 8,
+                    "d2h_bytes_per_step": (2 if log_h else 1) * E * S * 8 + S * 8},
+            "gpu_launches": K * (launches_fwd + launches_rev),
+            "roofline": {"bound": "hbm", "kernel": "k_reverse (reverse pass average per step)",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peak_kind, "bytes_per_step": b_rev},
+            "clocks": clocks.summary(t0, t1),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_batched(args):
     """64 uneven tubes (own resolution, radius, length, sample count and CFL time step)
     advanced by one persistent launch per step; metric summed over all tubes."""
@@ -420,6 +550,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched64":
         return run_batched(args)
+    if args.workload in ("adjoint64", "stenosed512x2048"):
+        return run_adjoint(args)
     return run_gpu(args)
 
 

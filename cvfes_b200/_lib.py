@@ -132,6 +132,8 @@ SIGNATURES = {
                                       C.POINTER(C.c_int32), P]),
     "cvfes_batch_graph_capture": (C.c_int, [P, I32, I64, I32, I32, P, I64, I32,
                                             C.POINTER(C.c_void_p)]),
+    "cvfes_set_adjoint_tuning": (C.c_int, [I32, I32, I32, I32, I32]),
+    "cvfes_get_adjoint_tuning": (C.c_int, [I32, P, P, P, P]),
     "cvfes_adjoint_ckpt_count": (C.c_int64, [I64, I64]),
     "cvfes_adjoint_jpart_size": (C.c_int64, [I64, I32, I32, I64]),
     "cvfes_adjoint_owner_blocks": (C.c_int, [DESC, I32, P, P, P, P]),
@@ -154,6 +156,16 @@ def get_step_tuning(precision: int) -> dict:
 
 def set_step_tuning(precision: int, vec: int, npb: int, staged: int, minb: int) -> None:
     call("cvfes_set_step_tuning", precision, vec, npb, staged, minb)
+
+
+def get_adjoint_tuning(precision: int) -> dict:
+    vals = [C.c_int32() for _ in range(4)]
+    call("cvfes_get_adjoint_tuning", precision, *[C.byref(v) for v in vals])
+    return dict(zip(("vec", "npb", "variant", "minb"), (v.value for v in vals)))
+
+
+def set_adjoint_tuning(precision: int, vec: int, npb: int, variant: int, minb: int) -> None:
+    call("cvfes_set_adjoint_tuning", precision, vec, npb, variant, minb)
 
 _lock = threading.Lock()
 _lib = None

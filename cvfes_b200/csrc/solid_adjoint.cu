@@ -163,6 +163,9 @@ struct RevArgs {
     T w0;
     int tpn;
     int npb;
+    int nch;        // sample chunks of 32*VEC per node block (fan kernel)
+    int cap_slots;  // slot capacity of the shared-memory stage (fan kernel)
+    int* status;    // bit 0: a bounded wait gave up; bit 1: stage too small
 };
 
 template <typename T>
@@ -186,8 +189,103 @@ __device__ __forceinline__ void load27(const T* K, T (&kk)[27]) {
     }
 }
 
+// Gamma_e += dchi^T Khat_e du for the element owned by this slot: (u1, u2) and (x1, x2) are
+// the first and second neighbour rows of u_n and chi_{n+1}, already differences
+// u_b - u_a in the DIFF form, raw rows otherwise.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, size_t S, size_t col,
+                                           const Vec<T, V> (&u1)[3], const Vec<T, V> (&u2)[3],
+                                           const Vec<T, V> (&x1)[3], const Vec<T, V> (&x2)[3],
+                                           const Vec<T, V> (&ua)[3], const Vec<T, V> (&ca)[3]) {
+    Vec<T, V> du1[3], du2[3], dy1[3], dy2[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if constexpr (DIFF) {
+            du1[d] = u1[d];
+            du2[d] = u2[d];
+            dy1[d] = x1[d];
+            dy2[d] = x2[d];
+        } else {
+            du1[d] = vsub(u1[d], ua[d]);
+            du2[d] = vsub(u2[d], ua[d]);
+            dy1[d] = vsub(x1[d], ca[d]);
+            dy2[d] = vsub(x2[d], ca[d]);
+        }
+    }
+    T ob[27];
+    load27<T>(A.own + (size_t)kOwnStride * e, ob);
+    Vec<T, V> g = vzero<T, V>();
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Vec<T, V> z1 = vzero<T, V>(), z2 = vzero<T, V>();
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+            axpy(z1, ob[3 * i + jj], du1[jj]);       // K_b1b1
+            axpy(z1, ob[9 + 3 * i + jj], du2[jj]);   // K_b1b2
+            axpy(z2, ob[9 + 3 * jj + i], du1[jj]);   // K_b2b1 = K_b1b2^T
+            axpy(z2, ob[18 + 3 * i + jj], du2[jj]);  // K_b2b2
+        }
+        vfma(g, dy1[i], z1);
+        vfma(g, dy2[i], z2);
+    }
+    T* gp = A.gam + (size_t)e * S + col;
+    Vec<T, V> gv = ld<T, V>(gp);
+#pragma unroll
+    for (int q = 0; q < V; ++q) gv.v[q] += g.v[q];
+    st<T, V>(gp, gv);
+}
+
+// Node update of one reverse step: u_{n-1} (backward step), chi_n, and G += chi_{n+1} . r_n.
+template <typename T, int V, bool GM>
+__device__ __forceinline__ void rev_epilogue(const RevArgs<T>& A, long long a, size_t S,
+                                             size_t col, size_t row, const Vec<T, V> (&ua)[3],
+                                             const Vec<T, V> (&ca)[3],
+                                             const Vec<T, V> (&accU)[3],
+                                             const Vec<T, V> (&accC)[3]) {
+    if (a < A.n_clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp), z = vzero<T, V>();
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            st<T, V>(A.uo + row + d * S, cl);
+            st<T, V>(A.xo + row + d * S, z);
+        }
+        return;
+    }
+    const T p = (T)A.p[0];
+    const Vec<T, V> im = ldg<T, V>(A.invm + (size_t)a * S + col);
+    Vec<T, V> gacc = vzero<T, V>();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T f = p * __ldg(A.fhat + 4 * a + d);
+        const Vec<T, V> u1 = ld<T, V>(A.uo + row + d * S);
+        const Vec<T, V> x2o = ld<T, V>(A.xo + row + d * S);
+        Vec<T, V> um, xn;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const bool live = im.v[i] != T(0);
+            const T w = A.w0 * im.v[i];
+            const T r = f - accU[d].v[i];
+            const T dv = ((u1.v[i] - ua[d].v[i]) - w * r) * A.inv1meta;
+            um.v[i] = live ? ua[d].v[i] - dv : T(0);
+            const T dx = ca[d].v[i] - x2o.v[i];
+            xn.v[i] = live ? ca[d].v[i] + fma(-A.eta, dx, dx) - w * accC[d].v[i] : T(0);
+            if constexpr (GM) gacc.v[i] = fma(ca[d].v[i], r, gacc.v[i]);
+        }
+        st<T, V>(A.uo + row + d * S, um);
+        st<T, V>(A.xo + row + d * S, xn);
+    }
+    if constexpr (GM) {
+        T* gp = A.gm + (size_t)a * S + col;
+        Vec<T, V> gv = ld<T, V>(gp);
+#pragma unroll
+        for (int q = 0; q < V; ++q) gv.v[q] += gacc.v[q];
+        st<T, V>(gp, gv);
+    }
+}
+
 // One reverse step for (node a, V samples): reconstruct u_{n-1}, advance chi, accumulate
-// Gamma over the elements this node owns and G of this node.
+// Gamma over the elements this node owns and G of this node.  Rows are gathered
+// through L1; a fan continuation reuses the previous slot's second neighbour.
 template <typename T, int V, bool DIFF, bool GM>
 __global__ void __launch_bounds__(256) k_reverse(RevArgs<T> A) {
     long long a;
@@ -202,7 +300,6 @@ __global__ void __launch_bounds__(256) k_reverse(RevArgs<T> A) {
         ua[d] = ldg<T, V>(A.u + row + d * S);
         ca[d] = ldg<T, V>(A.x + row + d * S);
     }
-    const T p = (T)A.p[0];
     Vec<T, V> accU[3], accC[3], cu[3], cc[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -269,89 +366,199 @@ __global__ void __launch_bounds__(256) k_reverse(RevArgs<T> A) {
             vfma(accU[i], c, tu);
             vfma(accC[i], c, tc);
         }
-        if (((r.w >> 8) & 3) == 0) {
-            // owner slot: Gamma_e += dchi^T Khat du over the two neighbours
-            Vec<T, V> du1[3], du2[3], dy1[3], dy2[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if constexpr (DIFF) {
-                    du1[d] = x1[d];
-                    du2[d] = x2[d];
-                    dy1[d] = y1[d];
-                    dy2[d] = y2[d];
-                } else {
-                    du1[d] = vsub(x1[d], ua[d]);
-                    du2[d] = vsub(x2[d], ua[d]);
-                    dy1[d] = vsub(y1[d], ca[d]);
-                    dy2[d] = vsub(y2[d], ca[d]);
-                }
-            }
-            T ob[27];
-            load27<T>(A.own + (size_t)kOwnStride * r.x, ob);
-            Vec<T, V> g = vzero<T, V>();
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                Vec<T, V> z1 = vzero<T, V>(), z2 = vzero<T, V>();
-#pragma unroll
-                for (int jj = 0; jj < 3; ++jj) {
-                    axpy(z1, ob[3 * i + jj], du1[jj]);        // K_b1b1
-                    axpy(z1, ob[9 + 3 * i + jj], du2[jj]);    // K_b1b2
-                    axpy(z2, ob[9 + 3 * jj + i], du1[jj]);    // K_b2b1 = K_b1b2^T
-                    axpy(z2, ob[18 + 3 * i + jj], du2[jj]);   // K_b2b2
-                }
-                vfma(g, dy1[i], z1);
-                vfma(g, dy2[i], z2);
-            }
-            T* gp = A.gam + (size_t)r.x * S + col;
-            Vec<T, V> gv = ld<T, V>(gp);
-#pragma unroll
-            for (int q = 0; q < V; ++q) gv.v[q] += g.v[q];
-            st<T, V>(gp, gv);
-        }
+        if (((r.w >> 8) & 3) == 0) owner_grad<T, V, DIFF>(A, r.x, S, col, x1, x2, y1, y2, ua, ca);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             cu[d] = x2[d];
             cc[d] = y2[d];
         }
     }
-    if (a < A.n_clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp), z = vzero<T, V>();
+    rev_epilogue<T, V, GM>(A, a, S, col, row, ua, ca, accU, accC);
+}
+
+// ------------------------------------------------------------ fan-rotation reverse step
+// As the forward fan kernel: a warp per node and 32*VEC-sample chunk, the block's slot
+// records and stiffness rows bulk-copied (TMA) into shared memory, and the neighbour
+// rows of u_n and chi_{n+1} rotating through three register sets so that the loads of
+// slot k+1 are in flight while slot k is multiplied.
+template <typename T, int V>
+__device__ __forceinline__ void load3(Vec<T, V> (&x)[3], const T* __restrict__ base, int node,
+                                      size_t S, size_t col) {
+    const T* p = base + (size_t)node * 3 * S + col;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            st<T, V>(A.uo + row + d * S, cl);
-            st<T, V>(A.xo + row + d * S, z);
+    for (int d = 0; d < 3; ++d) x[d] = ldg<T, V>(p + d * S);
+}
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void diff3(Vec<T, V> (&x)[3], const Vec<T, V> (&ref)[3]) {
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d] = vsub(x[d], ref[d]);
+    }
+}
+
+// Both row products of one slot from one read of its stiffness rows (shared memory).
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void slot_fma2(const T* K, const Vec<T, V>& c,
+                                          const Vec<T, V> (&u1)[3], const Vec<T, V> (&u2)[3],
+                                          const Vec<T, V> (&x1)[3], const Vec<T, V> (&x2)[3],
+                                          const Vec<T, V> (&ua)[3], const Vec<T, V> (&ca)[3],
+                                          Vec<T, V> (&accU)[3], Vec<T, V> (&accC)[3]) {
+    T kk[28];
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int q = (DIFF ? 2 : 0); q < 7; ++q) {
+            const float4 t = reinterpret_cast<const float4*>(K)[q];
+            kk[4 * q] = t.x;
+            kk[4 * q + 1] = t.y;
+            kk[4 * q + 2] = t.z;
+            kk[4 * q + 3] = t.w;
         }
+    } else {
+#pragma unroll
+        for (int q = (DIFF ? 4 : 0); q < 14; ++q) {
+            const double2 t = reinterpret_cast<const double2*>(K)[q];
+            kk[2 * q] = t.x;
+            kk[2 * q + 1] = t.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Vec<T, V> tu = vzero<T, V>(), tc = vzero<T, V>();
+        if constexpr (!DIFF) {
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) {
+                axpy(tu, kk[3 * i + jj], ua[jj]);
+                axpy(tc, kk[3 * i + jj], ca[jj]);
+            }
+        }
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+            axpy(tu, kk[9 + 3 * i + jj], u1[jj]);
+            axpy(tc, kk[9 + 3 * i + jj], x1[jj]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+            axpy(tu, kk[18 + 3 * i + jj], u2[jj]);
+            axpy(tc, kk[18 + 3 * i + jj], x2[jj]);
+        }
+        vfma(accU[i], c, tu);
+        vfma(accC[i], c, tc);
+    }
+}
+
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void rev_phase(int& k, int k1, const int4* srec, const T* sslab,
+                                          const RevArgs<T>& A, size_t S, size_t col,
+                                          const Vec<T, V> (&ua)[3], const Vec<T, V> (&ca)[3],
+                                          Vec<T, V> (&accU)[3], Vec<T, V> (&accC)[3],
+                                          Vec<T, V> (&pu)[3], Vec<T, V> (&px)[3],
+                                          Vec<T, V> (&cu)[3], Vec<T, V> (&cx)[3],
+                                          const Vec<T, V>& ccur, Vec<T, V> (&nu)[3],
+                                          Vec<T, V> (&nx)[3], Vec<T, V>& cnxt) {
+    const bool more = k + 1 < k1;
+    int4 rn = make_int4(0, 0, 0, 1);
+    if (more) {
+        rn = srec[k + 1];
+        load3<T, V>(nu, A.u, rn.z, S, col);
+        load3<T, V>(nx, A.x, rn.z, S, col);
+        cnxt = ldg<T, V>(A.coef + (size_t)rn.x * S + col);
+    }
+    diff3<T, V, DIFF>(cu, ua);
+    diff3<T, V, DIFF>(cx, ca);
+    const int4 r = srec[k];
+    slot_fma2<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, pu, cu, px, cx, ua, ca, accU,
+                          accC);
+    if (((r.w >> 8) & 3) == 0) owner_grad<T, V, DIFF>(A, r.x, S, col, pu, cu, px, cx, ua, ca);
+    if (more && !(rn.w & 1)) {  // fan break: the next slot's first neighbour is new
+        load3<T, V>(cu, A.u, rn.y, S, col);
+        load3<T, V>(cx, A.x, rn.y, S, col);
+        diff3<T, V, DIFF>(cu, ua);
+        diff3<T, V, DIFF>(cx, ca);
+    }
+    ++k;
+}
+
+template <typename T, int V, bool DIFF, bool GM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_reverse_fan(RevArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long nb = blockIdx.x / A.nch;
+    const int chunk = (int)(blockIdx.x - nb * A.nch);
+    const long long a0 = nb * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots) {
+        if (threadIdx.x == 0 && A.status) atomicOr(A.status, 2);
         return;
     }
-    const Vec<T, V> im = ldg<T, V>(A.invm + (size_t)a * S + col);
-    Vec<T, V> gacc = vzero<T, V>();
+    const uint32_t bar = smem_u32(smem);
+    int4* srec = reinterpret_cast<int4*>(smem + 16);
+    T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_rec = (uint32_t)nsl * 16u;
+        const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        if (nsl > 0) {
+            bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+            bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+        }
+    }
+    const long long a = a0 + warp;
+    const bool active = warp < A.npb && a < a1;
+    const size_t S = (size_t)A.S;
+    const size_t col = ((size_t)chunk * 32 + lane) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    Vec<T, V> ua[3], ca[3];
+    if (active) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ua[d] = ldg<T, V>(A.u + row + d * S);
+            ca[d] = ldg<T, V>(A.x + row + d * S);
+            prefetch_l2(A.uo + row + d * S);
+            prefetch_l2(A.xo + row + d * S);
+        }
+        prefetch_l2(A.invm + (size_t)a * S + col);
+    }
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        if (lane == 0 && A.status) atomicOr(A.status, 1);
+        return;
+    }
+    if (!active) return;
+    Vec<T, V> accU[3], accC[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const T f = p * __ldg(A.fhat + 4 * a + d);
-        const Vec<T, V> u1 = ld<T, V>(A.uo + row + d * S);
-        const Vec<T, V> x2o = ld<T, V>(A.xo + row + d * S);
-        Vec<T, V> um, xn;
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            const bool live = im.v[i] != T(0);
-            const T w = A.w0 * im.v[i];
-            const T r = f - accU[d].v[i];
-            const T dv = ((u1.v[i] - ua[d].v[i]) - w * r) * A.inv1meta;
-            um.v[i] = live ? ua[d].v[i] - dv : T(0);
-            const T dx = ca[d].v[i] - x2o.v[i];
-            xn.v[i] = live ? ca[d].v[i] + fma(-A.eta, dx, dx) - w * accC[d].v[i] : T(0);
-            if constexpr (GM) gacc.v[i] = fma(ca[d].v[i], r, gacc.v[i]);
+        accU[d] = vzero<T, V>();
+        accC[d] = vzero<T, V>();
+    }
+    const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+    if (k0 < k1) {
+        Vec<T, V> U0[3], U1[3], U2[3], X0[3], X1[3], X2[3], c0, c1, c2;
+        const int4 r0 = srec[k0];
+        load3<T, V>(U0, A.u, r0.y, S, col);
+        load3<T, V>(X0, A.x, r0.y, S, col);
+        load3<T, V>(U1, A.u, r0.z, S, col);
+        load3<T, V>(X1, A.x, r0.z, S, col);
+        c1 = ldg<T, V>(A.coef + (size_t)r0.x * S + col);
+        diff3<T, V, DIFF>(U0, ua);
+        diff3<T, V, DIFF>(X0, ca);
+        int k = k0;
+        while (true) {
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U0, X0, U1,
+                                  X1, c1, U2, X2, c2);
+            if (k >= k1) break;
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U1, X1, U2,
+                                  X2, c2, U0, X0, c0);
+            if (k >= k1) break;
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U2, X2, U0,
+                                  X0, c0, U1, X1, c1);
+            if (k >= k1) break;
         }
-        st<T, V>(A.uo + row + d * S, um);
-        st<T, V>(A.xo + row + d * S, xn);
     }
-    if constexpr (GM) {
-        T* gp = A.gm + (size_t)a * S + col;
-        Vec<T, V> gv = ld<T, V>(gp);
-#pragma unroll
-        for (int q = 0; q < V; ++q) gv.v[q] += gacc.v[q];
-        st<T, V>(gp, gv);
-    }
+    rev_epilogue<T, V, GM>(A, a, S, col, row, ua, ca, accU, accC);
 }
 
 // dJ/dlogE = -c Gamma; dJ/dlogh = -c Gamma - h sum_a alpha_{e,a} G_a / m_a.
@@ -385,6 +592,61 @@ __global__ void k_grad_final(long long n_elems, int S, const int32_t* __restrict
     }
 }
 
+struct RevTuning {
+    int vec;      // samples per thread (upper bound)
+    int npb;      // nodes (warps) per block of the fan kernel
+    int variant;  // 0: L1-gather kernel; 1: fan-rotation kernel with staged slots
+    int minb;     // resident blocks per SM asked of the compiler (fan kernel)
+};
+// Defaults from sweeps on the 256x1024 tube (FP32 128 samples, FP64 64 samples) on B200.
+static RevTuning g_rev32 = {2, 2, 1, 2};
+static RevTuning g_rev64 = {2, 2, 1, 1};
+template <typename T>
+RevTuning& rev_tuning() {
+    return sizeof(T) == 4 ? g_rev32 : g_rev64;
+}
+
+constexpr size_t kRevMaxStage = 160 * 1024;
+
+template <typename Kern, typename T>
+int launch_rev_fan(Kern kernel, unsigned grid, int threads, size_t smem, cudaStream_t st,
+                   const RevArgs<T>& A) {
+    if (smem > 48 * 1024) {
+        cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return fail(CVFES_ERR_CUDA, "k_reverse_fan smem attribute: %s", cudaGetErrorString(e));
+    }
+    kernel<<<grid, threads, smem, st>>>(A);
+    CVFES_LAUNCH_CHECK("k_reverse_fan");
+    return CVFES_OK;
+}
+
+template <typename T, int V, bool DIFF, bool GM>
+int launch_rev_fan_m(int minb, unsigned grid, int threads, size_t smem, cudaStream_t st,
+                     const RevArgs<T>& A) {
+    switch (minb) {
+        case 4: return launch_rev_fan(k_reverse_fan<T, V, DIFF, GM, 4>, grid, threads, smem, st, A);
+        case 3: return launch_rev_fan(k_reverse_fan<T, V, DIFF, GM, 3>, grid, threads, smem, st, A);
+        case 2: return launch_rev_fan(k_reverse_fan<T, V, DIFF, GM, 2>, grid, threads, smem, st, A);
+        default: return launch_rev_fan(k_reverse_fan<T, V, DIFF, GM, 1>, grid, threads, smem, st, A);
+    }
+}
+
+template <typename T, int V, bool DIFF>
+int launch_rev_v(const RevTuning& tu, bool fan, bool gmv, unsigned fan_grid, size_t smem,
+                 const RowGrid& rg, cudaStream_t st, const RevArgs<T>& A) {
+    if (fan) {
+        const int threads = 32 * tu.npb;
+        return gmv ? launch_rev_fan_m<T, V, DIFF, true>(tu.minb, fan_grid, threads, smem, st, A)
+                   : launch_rev_fan_m<T, V, DIFF, false>(tu.minb, fan_grid, threads, smem, st, A);
+    }
+    if (gmv) k_reverse<T, V, DIFF, true><<<rg.grid, 256, 0, st>>>(A);
+    else k_reverse<T, V, DIFF, false><<<rg.grid, 256, 0, st>>>(A);
+    CVFES_LAUNCH_CHECK("k_reverse");
+    return CVFES_OK;
+}
+
 template <typename T>
 int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T* x, T* xo,
                         long long n, cudaStream_t st) {
@@ -408,40 +670,48 @@ int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T*
     A.S = (int)m->n_samples;
     A.n_clamped = (int)m->n_clamped;
     A.clamp = (T)m->clamp_value;
+    A.status = m->status;
     const double g = 0.5 * d->dt * d->damp;
     const double eta = d->dt * d->damp / (1.0 + g);
     A.eta = (T)eta;
     A.inv1meta = (T)(1.0 / (1.0 - eta));
     A.w0 = (T)(d->dt * d->dt / (1.0 + g));
+    const RevTuning tu = rev_tuning<T>();
     const void* ptrs[8] = {d->coef, d->invm, u, uo, x, xo, d->gamma, d->gmass};
-    const int maxv = (int)(16 / sizeof(T));
-    int V = maxv;
+    int V = (int)(16 / sizeof(T));
+    while (V > tu.vec) V /= 2;
     for (; V > 1; V /= 2) {
         bool ok = A.S % V == 0;
         for (int i = 0; i < 8; ++i)
             if (ptrs[i] && reinterpret_cast<uintptr_t>(ptrs[i]) % (V * sizeof(T))) ok = false;
         if (ok) break;
     }
-    const int block = 256;
-    const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
+    const RowGrid rg = row_grid(m->n_nodes, A.S / V, 256);
     A.tpn = rg.tpn;
     A.npb = rg.npb;
+    A.nch = 1;
+    A.cap_slots = 0;
+    const long long cap = (long long)tu.npb * m->max_degree;
+    const size_t smem = 16 + (size_t)cap * (16 + kSlabStride * sizeof(T));
+    const bool fan = tu.variant == 1 && m->max_degree > 0 && (A.S / V) % 32 == 0 &&
+                     smem <= kRevMaxStage && tu.npb >= 1 && tu.npb <= 8;
+    unsigned fan_grid = 0;
+    if (fan) {
+        A.npb = tu.npb;
+        A.tpn = 32;
+        A.nch = A.S / V / 32;
+        A.cap_slots = (int)cap;
+        fan_grid = (unsigned)(((m->n_nodes + A.npb - 1) / A.npb) * A.nch);
+    }
     constexpr bool DIFF = std::is_same<T, float>::value;
     const bool gmv = d->gmass != nullptr;
     if (V == 4) {
-        if constexpr (sizeof(T) == 4) {
-            if (gmv) k_reverse<T, 4, DIFF, true><<<rg.grid, block, 0, st>>>(A);
-            else k_reverse<T, 4, DIFF, false><<<rg.grid, block, 0, st>>>(A);
-        }
-    } else if (V == 2) {
-        if (gmv) k_reverse<T, 2, DIFF, true><<<rg.grid, block, 0, st>>>(A);
-        else k_reverse<T, 2, DIFF, false><<<rg.grid, block, 0, st>>>(A);
-    } else {
-        if (gmv) k_reverse<T, 1, DIFF, true><<<rg.grid, block, 0, st>>>(A);
-        else k_reverse<T, 1, DIFF, false><<<rg.grid, block, 0, st>>>(A);
+        if constexpr (sizeof(T) == 4)
+            return launch_rev_v<T, 4, DIFF>(tu, fan, gmv, fan_grid, smem, rg, st, A);
+        return fail(CVFES_ERR_UNSUPPORTED, "k_reverse: vec 4 is FP32 only");
     }
-    CVFES_LAUNCH_CHECK("k_reverse");
-    return CVFES_OK;
+    if (V == 2) return launch_rev_v<T, 2, DIFF>(tu, fan, gmv, fan_grid, smem, rg, st, A);
+    return launch_rev_v<T, 1, DIFF>(tu, fan, gmv, fan_grid, smem, rg, st, A);
 }
 
 int check_adjoint(const cvfes_adjoint_desc* d, const char* who) {
@@ -626,6 +896,29 @@ int capture(F&& issue, cvfes_graph** out) {
 }  // namespace cvfes
 
 using namespace cvfes;
+
+extern "C" int cvfes_set_adjoint_tuning(int32_t precision, int32_t vec, int32_t npb,
+                                        int32_t variant, int32_t minb) {
+    if ((precision != 32 && precision != 64) || (vec != 1 && vec != 2 && vec != 4) ||
+        (precision == 64 && vec == 4) || npb < 1 || npb > 8 || variant < 0 || variant > 1 ||
+        minb < 1 || minb > 4)
+        return fail(CVFES_ERR_ARG, "cvfes_set_adjoint_tuning: bad argument");
+    RevTuning& t = precision == 32 ? g_rev32 : g_rev64;
+    t = RevTuning{vec, npb, variant, minb};
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_get_adjoint_tuning(int32_t precision, int32_t* vec, int32_t* npb,
+                                        int32_t* variant, int32_t* minb) {
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_get_adjoint_tuning: precision must be 32 or 64");
+    const RevTuning& t = precision == 32 ? g_rev32 : g_rev64;
+    if (vec) *vec = t.vec;
+    if (npb) *npb = t.npb;
+    if (variant) *variant = t.variant;
+    if (minb) *minb = t.minb;
+    return CVFES_OK;
+}
 
 extern "C" int64_t cvfes_adjoint_ckpt_count(int64_t n_steps, int64_t ckpt_every) {
     if (n_steps <= 0 || ckpt_every <= 0) return 0;

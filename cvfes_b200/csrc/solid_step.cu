@@ -438,6 +438,108 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
 }
 
+// ------------------------------------------------------------ burst-gather step
+// As k_step_fan (TMA-staged slot rows, a warp per node and sample chunk), but every
+// neighbour row of the node and every element coefficient row is requested at once,
+// before any product: the node's whole gather (deg + 1 row sets and deg coefficient
+// rows, deg <= MAXD) is in flight together, which raises the bytes in flight per SM
+// over the fan kernel's one-element lookahead.  Neighbour row j+1 is the second
+// neighbour of slot j and the first of slot j+1 (fan order); a fan break past slot 0
+// loads its first neighbour when the slot is multiplied.
+template <typename T, int V, bool DIFF, int MAXD, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_burst(StepArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long nb = blockIdx.x / A.nch;
+    const int chunk = (int)(blockIdx.x - nb * A.nch);
+    const long long a0 = nb * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots) {
+        if (threadIdx.x == 0 && A.status) atomicOr(A.status, 2);
+        return;
+    }
+    const uint32_t bar = smem_u32(smem);
+    int4* srec = reinterpret_cast<int4*>(smem + 16);
+    T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_rec = (uint32_t)nsl * 16u;
+        const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        if (nsl > 0) {
+            bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+            bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+        }
+    }
+    const long long a = a0 + warp;
+    const bool active = warp < A.npb && a < a1;
+    const size_t S = (size_t)A.S;
+    const size_t col = ((size_t)chunk * 32 + lane) * V;
+    const size_t row = (size_t)a * 3 * S + col;
+    const bool clamped = a < A.n_clamped;
+    Vec<T, V> ua[3];
+    T f[3];
+    if (active && !clamped) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ua[d] = ldg<T, V>(A.u + row + d * S);
+            prefetch_l2(A.up + row + d * S);
+        }
+        prefetch_l2(A.invm + (size_t)a * S + col);
+        node_load<T>(A, a, step_pressure<T>(A), f);
+    }
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        if (lane == 0 && A.status) atomicOr(A.status, 1);
+        return;
+    }
+    if (!active) return;
+    if (clamped) {
+        const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        return;
+    }
+    const int k0 = __ldg(A.node_ptr + a) - kb;
+    const int deg = __ldg(A.node_ptr + a + 1) - kb - k0;
+    Vec<T, V> R[MAXD + 1][3];
+    Vec<T, V> C[MAXD];
+    if (deg > 0) load_rows<T, V>(R[0], A.u, srec[k0].y, S, col);
+#pragma unroll
+    for (int j = 0; j < MAXD; ++j) {
+        if (j < deg) {
+            const int4 r = srec[k0 + j];
+            load_rows<T, V>(R[j + 1], A.u, r.z, S, col);
+            C[j] = ldg<T, V>(A.coef + (size_t)r.x * S + col);
+        }
+    }
+    Vec<T, V> acc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    if (deg > 0) to_diff<T, V, DIFF>(R[0], ua);
+#pragma unroll
+    for (int j = 0; j < MAXD; ++j) {
+        if (j < deg) {
+            to_diff<T, V, DIFF>(R[j + 1], ua);
+            const int4 r = srec[k0 + j];
+            if (j > 0 && !(r.w & 1)) {  // fan break: a first neighbour of its own
+                Vec<T, V> b1[3];
+                load_rows<T, V>(b1, A.u, r.y, S, col);
+                to_diff<T, V, DIFF>(b1, ua);
+                slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * (k0 + j), C[j], b1, R[j + 1],
+                                     ua, acc);
+            } else {
+                slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * (k0 + j), C[j], R[j], R[j + 1],
+                                     ua, acc);
+            }
+        }
+    }
+    step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+}
+
 // ------------------------------------------------------------ pipelined persistent step
 // Persistent kernel: every warp owns a private STAGES-deep ring of shared-memory
 // stages and walks its own sequence of work items (node, 32*VEC-sample chunk;
@@ -985,10 +1087,26 @@ int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, 
     }
 }
 
+template <typename T, int V, bool DIFF, int MAXD>
+int launch_burst(int minb, dim3 g1, int threads, size_t smem, cudaStream_t st,
+                 const StepArgs<T>& A) {
+    switch (minb) {
+        case 4: return launch_staged(k_step_burst<T, V, DIFF, MAXD, 4>, g1, threads, smem, st, A);
+        case 3: return launch_staged(k_step_burst<T, V, DIFF, MAXD, 3>, g1, threads, smem, st, A);
+        case 2: return launch_staged(k_step_burst<T, V, DIFF, MAXD, 2>, g1, threads, smem, st, A);
+        default: return launch_staged(k_step_burst<T, V, DIFF, MAXD, 1>, g1, threads, smem, st, A);
+    }
+}
+
 template <typename T, int V, bool DIFF>
 int launch_staged_v(int variant, int minb, dim3 grid, int threads, size_t smem, cudaStream_t st,
-                    const StepArgs<T>& A) {
-    if (variant == 3) {
+                    const StepArgs<T>& A, long long max_degree = 0) {
+    if (variant == 5 && max_degree > 0 && max_degree <= 8) {
+        const dim3 g1((unsigned)((long long)grid.x * grid.y));
+        if (max_degree <= 6) return launch_burst<T, V, DIFF, 6>(minb, g1, threads, smem, st, A);
+        return launch_burst<T, V, DIFF, 8>(minb, g1, threads, smem, st, A);
+    }
+    if (variant == 3 || variant == 5) {
         const dim3 g1((unsigned)((long long)grid.x * grid.y));
         switch (minb) {
             case 4: return launch_staged(k_step_fan<T, V, DIFF, 4>, g1, threads, smem, st, A);
@@ -1085,11 +1203,13 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
         if (V == 4) {
             if constexpr (sizeof(T) == 4)
                 rc = launch_staged_v<T, 4, DIFF>(tune.staged, tune.minb, grid, threads, smem, st,
-                                                 A);
+                                                 A, m->max_degree);
         } else if (V == 2) {
-            rc = launch_staged_v<T, 2, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A);
+            rc = launch_staged_v<T, 2, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A,
+                                             m->max_degree);
         } else {
-            rc = launch_staged_v<T, 1, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A);
+            rc = launch_staged_v<T, 1, DIFF>(tune.staged, tune.minb, grid, threads, smem, st, A,
+                                             m->max_degree);
         }
         return rc;
     }
@@ -1384,11 +1504,11 @@ extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: npb must be in 1..8");
     if (minb < 1 || minb > 4)
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: minb must be in 1..4");
+    if (staged < 0 || staged > 5)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..5");
     StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
     t.vec = vec;
     t.npb = npb;
-    if (staged < 0 || staged > 4)
-        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..4");
     t.staged = staged;
     t.minb = minb;
     return CVFES_OK;

@@ -21,8 +21,9 @@ import torch
 from . import _lib
 
 STEP_CANDIDATES = {
-    32: [(3, 4, 2, 2), (3, 4, 4, 2), (3, 4, 2, 1), (1, 4, 4, 2), (3, 2, 2, 3), (0, 4, 8, 1)],
-    64: [(3, 2, 2, 2), (3, 2, 4, 2), (1, 2, 4, 2), (3, 1, 4, 3), (0, 2, 8, 1)],
+    32: [(3, 4, 2, 2), (3, 4, 4, 2), (3, 4, 2, 1), (1, 4, 4, 2), (3, 2, 2, 3), (5, 4, 2, 1),
+         (0, 4, 8, 1)],
+    64: [(3, 2, 2, 2), (3, 2, 4, 2), (1, 2, 4, 2), (3, 1, 4, 3), (5, 1, 2, 2), (0, 2, 8, 1)],
 }
 
 

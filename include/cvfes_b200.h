@@ -74,6 +74,9 @@ typedef struct cvfes_solid_mesh {
  *           4 = persistent pipelined kernel: each warp streams its own work
  *               items through a ring of `minb` (2..4) shared-memory stages
  *               (rows by cp.async, slot rows by TMA); npb = warps per block;
+ *           5 = as 1, with the node's whole gather (every neighbour row and
+ *               coefficient row) requested before the first product (meshes of
+ *               node degree <= 8; otherwise as 3);
  *   minb: resident blocks per SM the register allocation must allow (1..4).
  * Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,
@@ -338,6 +341,14 @@ typedef struct cvfes_adjoint_desc {
     double       damp;
 } cvfes_adjoint_desc;
 
+/* Reverse-step kernel choice per precision: samples per thread (1|2|4, FP64 1|2),
+ * nodes per block (1..8), variant (0: L1 gather, 1: fan rotation with TMA-staged
+ * slot rows, needing S/vec a multiple of 32), minimum blocks per SM (1..4, a register
+ * cap).  Every choice gives bitwise the same results. */
+int cvfes_set_adjoint_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t variant,
+                             int32_t minb);
+int cvfes_get_adjoint_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t* variant,
+                             int32_t* minb);
 int64_t cvfes_adjoint_ckpt_count(int64_t n_steps, int64_t ckpt_every);
 int64_t cvfes_adjoint_jpart_size(int64_t n_steps, int32_t obs_every, int32_t n_obs,
                                  int64_t n_samples);

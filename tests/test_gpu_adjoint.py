@@ -133,3 +133,29 @@ def test_problem_rejects_bad_observation_nodes(lib, cuda):
         MismatchProblem(mesh, case_dt(SMALL, mesh), np.zeros(20), [3, 3], device=cuda)
     with pytest.raises(ValueError):
         MismatchProblem(mesh, case_dt(SMALL, mesh), np.zeros(20), [mesh.nNodes], device=cuda)
+
+
+REV_VARIANTS = {
+    32: [(4, 8, 0, 1), (2, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 2), (4, 2, 1, 1), (2, 4, 1, 2)],
+    64: [(2, 8, 0, 1), (1, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 1), (2, 4, 1, 2)],
+}
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_reverse_kernel_variants_are_bitwise_identical(lib, cuda, precision):
+    """L1-gather and fan-rotation reverse kernels, every tile shape: same bits."""
+    from cvfes_b200 import _lib
+    case = dataclasses.replace(SMALL, n_samples=128 if precision == 32 else 64)
+    p, logE, logh, _ = adjoint_setup(case, precision=precision, device=cuda, grad_logh=True)
+    saved = _lib.get_adjoint_tuning(precision)
+    outs = []
+    try:
+        for tune in REV_VARIANTS[precision]:
+            _lib.set_adjoint_tuning(precision, *tune)
+            p.release_graphs()
+            p.objective(logE, logh)
+            outs.append(p.gradient())
+    finally:
+        _lib.set_adjoint_tuning(precision, **saved)
+    for tune, (gE, gh) in zip(REV_VARIANTS[precision][1:], outs[1:]):
+        assert torch.equal(gE, outs[0][0]) and torch.equal(gh, outs[0][1]), tune

@@ -275,3 +275,25 @@ def test_partial_sample_chunks_against_oracle(lib, cuda, S):
                                graph_chunk=12)
         b.Advance(pres)
         assert so.rel_l2(b.displacement(0), o.u) < tol
+
+
+def test_burst_step_variant_matches_fan(lib, cuda):
+    """The burst-gather step kernel gives the fan kernel's bits (FP32 and FP64)."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    pres = case.pressures(36)
+    for precision, S, tunes in ((32, 128, [(4, 2, 3, 2), (4, 2, 5, 1), (2, 2, 5, 2)]),
+                                (64, 64, [(2, 2, 3, 2), (2, 2, 5, 1), (1, 2, 5, 2)])):
+        mesh = c0_mesh(S)
+        saved = _lib.get_step_tuning(precision)
+        outs = []
+        try:
+            for vec, npb, staged, minb in tunes:
+                _lib.set_step_tuning(precision, vec, npb, staged, minb)
+                s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+                s.Advance(pres)
+                outs.append(s.local_displacement().clone())
+        finally:
+            _lib.set_step_tuning(precision, **saved)
+        for o in outs[1:]:
+            assert torch.equal(o, outs[0])
