@@ -112,6 +112,9 @@ class GPUSolidSolver(PhysicsSolver):
         self.constant_T = getattr(config, "constant_T", 1.0)
         self.constantPressure = getattr(config, "constant_pressure", 0.0)
         self.pressure_ramp = getattr(config, "pressure_ramp", "cosine")
+        # stiffness_update_interval (cvconfig.py:154): 0 keeps the undeformed stiffness and
+        # load (linear templates); n >= 1 rebuilds both on x + u every n steps
+        self.update_interval = int(getattr(config, "update_interval", 0) or 0)
         self.nt = 0
         if self.stressFilename is not None:
             if self.useConstantStress:
@@ -196,6 +199,18 @@ class GPUSolidSolver(PhysicsSolver):
             self._graphs = {}
             self._p_buf = None
             self.step_count = 0
+            self.geo_counter = 0
+            self.geo_live = False
+            self.slot_geo = self.ugeo = None
+            if self.update_interval > 0:
+                gdt = torch.float64 if self.precision == 64 else torch.float32
+                self.slot_geo = torch.empty(8 * 3 * self.plan.E, dtype=gdt, device=dev)
+                g64 = self.slot_geo if self.precision == 64 else None
+                g32 = self.slot_geo if self.precision == 32 else None
+                call("cvfes_solid_slot_geometry_f64", self.plan.E, ptr(self.plan.nodes),
+                     ptr(self.plan.elems), ptr(self.plan.slot_rec), ptr(g64), ptr(g32),
+                     self._stream())
+                self.ugeo = torch.zeros((ndof, S), dtype=dtype, device=dev)
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -232,8 +247,36 @@ class GPUSolidSolver(PhysicsSolver):
         dtype = torch.float64 if self.precision == 64 else torch.float32
         self.trac_dev = torch.from_numpy(tr).to(self.device, dtype)
 
+    def _solve_geo(self, dt):
+        """One step on the deformed geometry with the reference's update counter
+        (``physicsSolver.py:296-324``; every step for interval 1, as assemble_K_P)."""
+        if self.trac_dev is not None:
+            raise NotImplementedError("nodal traction input is not supported with a "
+                                      "stiffness update interval")
+        if self.geo_counter >= self.update_interval:
+            if self.update_interval == 1:
+                self.geo_live = True
+            else:
+                self.ugeo.copy_(self.bufs[self.cur])
+            self.geo_counter = 1
+        else:
+            self.geo_counter += 1
+        ug = self.bufs[self.cur] if self.geo_live else self.ugeo
+        fn = "cvfes_solid_step_geo_f64" if self.precision == 64 else "cvfes_solid_step_geo_f32"
+        call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
+             ptr(self.plan.invm(self.precision)), ptr(self.slot_geo), ptr(self.bufs[self.cur]),
+             ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), ptr(ug), None, None, 0,
+             float(self.pressure), float(self.mesh.v), float(dt), float(self.damp),
+             self._stream())
+
     def Solve(self, t, dt):
         """One explicit step for all samples (``physicsSolverSDampGPUs.py:325-399``)."""
+        if self.update_interval > 0:
+            with torch.cuda.device(self.device):
+                self._solve_geo(dt)
+            self.prev, self.cur, self.nxt = self.cur, self.nxt, self.prev
+            self.step_count += 1
+            return
         fn = "cvfes_solid_step_f64" if self.precision == 64 else "cvfes_solid_step_f32"
         with torch.cuda.device(self.device):
             call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
@@ -255,6 +298,8 @@ class GPUSolidSolver(PhysicsSolver):
         p = self._schedule(pressures)
         n = int(p.numel())
         prec = self.precision
+        if self.update_interval > 0:
+            return self._advance_geo(p, n, dt)
         with torch.cuda.device(self.device):
             self.clock.zero_()
             done = 0
@@ -296,6 +341,32 @@ class GPUSolidSolver(PhysicsSolver):
                     self.cur, self.prev = order[cur_idx.value], order[prev_idx.value]
                     self.nxt = 3 - self.cur - self.prev
             self.step_count += n
+        return self
+
+    def _advance_geo(self, p, n, dt):
+        """Geometric steps as plain launches (the geometry update counter is host state)."""
+        if self.trac_dev is not None:
+            raise NotImplementedError("nodal traction input is not supported with a "
+                                      "stiffness update interval")
+        fn = "cvfes_solid_advance_geo_f64" if self.precision == 64 else \
+            "cvfes_solid_advance_geo_f32"
+        b = self.bufs
+        order = [self.cur, self.prev, self.nxt]
+        cur_idx, prev_idx, live = _lib.C.c_int32(), _lib.C.c_int32(), _lib.C.c_int32()
+        counter = _lib.C.c_int64(self.geo_counter)
+        with torch.cuda.device(self.device):
+            self.clock.zero_()
+            call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
+                 ptr(self.plan.invm(self.precision)), ptr(self.slot_geo), ptr(b[order[0]]),
+                 ptr(b[order[1]]), ptr(b[order[2]]), ptr(self.ugeo), ptr(p), ptr(self.clock), n,
+                 self.update_interval, _lib.C.byref(counter), int(self.geo_live),
+                 float(self.mesh.v), float(dt), float(self.damp), _lib.C.byref(cur_idx),
+                 _lib.C.byref(prev_idx), _lib.C.byref(live), self._stream())
+        self.cur, self.prev = order[cur_idx.value], order[prev_idx.value]
+        self.nxt = 3 - self.cur - self.prev
+        self.geo_counter = counter.value
+        self.geo_live = bool(live.value)
+        self.step_count += n
         return self
 
     def _schedule(self, pressures) -> torch.Tensor:

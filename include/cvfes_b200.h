@@ -300,6 +300,50 @@ int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, int64_t t
                               int32_t precision, int32_t vec, int64_t* clock, int64_t chunk,
                               int32_t grid, cvfes_graph** out);
 
+/* ------------------------------------------------------------ geometric update
+ * Stiffness and follower pressure on the deformed geometry x + u_g of each sample:
+ * the matrix-free K(x+u_g) u and p * sum_e (A_e/3) n_e of assemble_K_P
+ * (physicsSolverSDampGPUs.cl:232-393, every step) and of OptimizedSolidAssembleUpdate
+ * (optimizedSolidAssemble.pyx:710-819, every stiffness_update_interval steps,
+ * physicsSolver.py:296-324).  The update of the state is cvfes_solid_step's.
+ * slot_geo: [8 * 3E] per slot X_b1 - X_a, X_b2 - X_a (reference coordinates), from
+ * cvfes_solid_slot_geometry_f64 (nodes device f64 [N][3], elems device int32 [E][3]).
+ * ug: geometry displacement [3N][S] (NULL or == u: the current state).
+ * nu: Poisson ratio of D (physicsSolver.py:184-188, shear factor 5/6).          */
+int cvfes_solid_slot_geometry_f64(int64_t n_elems, const double* nodes, const int32_t* elems,
+                                  const int32_t* slot_rec, double* geo64, float* geo32,
+                                  void* stream);
+int cvfes_solid_step_geo_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
+                             const double* slot_geo, const double* u, const double* up,
+                             double* un, const double* ug, const double* p_sched,
+                             const int64_t* clock, int64_t j, double pressure, double nu,
+                             double dt, double damp, void* stream);
+int cvfes_solid_step_geo_f32(const cvfes_solid_mesh* mesh, const float* coef, const float* invm,
+                             const float* slot_geo, const float* u, const float* up, float* un,
+                             const float* ug, const double* p_sched, const int64_t* clock,
+                             int64_t j, double pressure, double nu, double dt, double damp,
+                             void* stream);
+/* n_steps geometric steps with the reference's update counter (physicsSolver.py:299-324):
+ * before each step, if *counter >= interval the geometry becomes the current state and
+ * *counter = 1, else *counter += 1.  interval 1 reads the geometry straight from u_n
+ * (geo_live tells whether that was already so before the call); larger intervals copy
+ * u_n into ugeo (caller-owned [3N][S], zeros = undeformed at the start).  Buffers
+ * rotate as in cvfes_solid_advance; *counter and *geo_live_out carry the state on. */
+int cvfes_solid_advance_geo_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                const double* invm, const double* slot_geo, double* buf0,
+                                double* buf1, double* buf2, double* ugeo, const double* p_sched,
+                                int64_t* clock, int64_t n_steps, int64_t interval,
+                                int64_t* counter, int32_t geo_live, double nu, double dt,
+                                double damp, int32_t* cur_idx, int32_t* prev_idx,
+                                int32_t* geo_live_out, void* stream);
+int cvfes_solid_advance_geo_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                const float* invm, const float* slot_geo, float* buf0,
+                                float* buf1, float* buf2, float* ugeo, const double* p_sched,
+                                int64_t* clock, int64_t n_steps, int64_t interval,
+                                int64_t* counter, int32_t geo_live, double nu, double dt,
+                                double damp, int32_t* cur_idx, int32_t* prev_idx,
+                                int32_t* geo_live_out, void* stream);
+
 /* ------------------------------------------------------------ adjoint
  * Gradient of the displacement-mismatch objective
  *     J_s = sum_{n % obs_every == 0, 0 < n <= T} sum_{i in obs} |u_n(i) - uobs_n(i)|^2

@@ -228,6 +228,55 @@ def template_multiply(elements, Kt, coefK, u):
     return out.reshape(N3, S)
 
 
+def geometric_update(nodes, elements, v, u):
+    """Restatement of ``OptimizedSolidAssembleUpdate`` (pyx:710-819) with unit traction, per
+    sample on the coordinates ``x + u_s`` (``mesh.py:678-680``): the unit stiffness of every
+    element per sample (S,E,9,9) and the unit follower load (3N, S).  Same steps as
+    ``element_frames`` / ``element_templates``, batched over samples."""
+    N = nodes.shape[0]
+    S = u.shape[1]
+    E = elements.shape[0]
+    xs = nodes[None] + u.T.reshape(S, N, 3)
+    p = xs[:, elements]                                   # (S,E,3,3): sample, elem, node, xyz
+    e0 = p[:, :, 2] - p[:, :, 1]
+    e1 = p[:, :, 0] - p[:, :, 2]
+    T = np.empty((S, E, 3, 3))
+    T[:, :, 0] = e0 / np.sqrt(np.sum(e0 * e0, axis=-1))[..., None]
+    proj = np.sum(e1 * T[:, :, 0], axis=-1)
+    t1 = e1 - proj[..., None] * T[:, :, 0]
+    T[:, :, 1] = t1 / np.sqrt(np.sum(t1 * t1, axis=-1))[..., None]
+    T[:, :, 2, 0] = T[:, :, 0, 1] * T[:, :, 1, 2] - T[:, :, 0, 2] * T[:, :, 1, 1]
+    T[:, :, 2, 1] = T[:, :, 0, 2] * T[:, :, 1, 0] - T[:, :, 0, 0] * T[:, :, 1, 2]
+    T[:, :, 2, 2] = T[:, :, 0, 0] * T[:, :, 1, 1] - T[:, :, 0, 1] * T[:, :, 1, 0]
+    lx = np.einsum("senk,sek->sen", p, T[:, :, 0])
+    ly = np.einsum("senk,sek->sen", p, T[:, :, 1])
+    area = ((lx[..., 1] * ly[..., 2] - lx[..., 2] * ly[..., 1])
+            - (lx[..., 0] * ly[..., 2] - lx[..., 2] * ly[..., 0])
+            + (lx[..., 0] * ly[..., 1] - lx[..., 1] * ly[..., 0])) * 0.5
+    y23, y31, y12 = ly[..., 1] - ly[..., 2], ly[..., 2] - ly[..., 0], ly[..., 0] - ly[..., 1]
+    x32, x13, x21 = lx[..., 2] - lx[..., 1], lx[..., 0] - lx[..., 2], lx[..., 1] - lx[..., 0]
+    c1 = 2.0 * area
+    B = np.zeros((S, E, 5, 9))
+    for (r, c), val in {(0, 0): y23, (2, 1): y23, (3, 2): y23,
+                        (0, 3): y31, (2, 4): y31, (3, 5): y31,
+                        (0, 6): y12, (2, 7): y12, (3, 8): y12,
+                        (1, 1): x32, (2, 0): x32, (4, 2): x32,
+                        (1, 4): x13, (2, 3): x13, (4, 5): x13,
+                        (1, 7): x21, (2, 6): x21, (4, 8): x21}.items():
+        B[:, :, r, c] = val / c1
+    Bt = np.swapaxes(B, -1, -2)
+    btdb = (Bt @ d_matrix(v)) @ B * area[..., None, None]
+    TT = np.zeros((S, E, 9, 9))
+    for a in range(3):
+        TT[:, :, 3 * a:3 * a + 3, 3 * a:3 * a + 3] = T
+    Kt = np.swapaxes(TT, -1, -2) @ btdb @ TT
+    f = np.zeros((N, 3, S))
+    load = (area / 3.0)[..., None] * T[:, :, 2]           # (S,E,3)
+    for a in range(3):
+        np.add.at(f, elements[:, a], load.transpose(1, 2, 0))
+    return Kt, f.reshape(3 * N, S)
+
+
 # --------------------------------------------------------------------------------------
 # Load schedules (RefreshContext semantics)
 # --------------------------------------------------------------------------------------
@@ -255,7 +304,7 @@ class OracleSolidSolver:
     """
 
     def __init__(self, nodes, elements, boundary, coefK, elmGThick, density, v, damp, dt,
-                 u0=None, du0=None, bdyU=0.0, p0=0.0, backend="numpy"):
+                 u0=None, du0=None, bdyU=0.0, p0=0.0, backend="numpy", update_interval=0):
         self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
         self.elements = np.ascontiguousarray(elements, dtype=np.int64)
         self.N = self.nodes.shape[0]
@@ -263,6 +312,12 @@ class OracleSolidSolver:
         self.dt = float(dt)
         self.bdyU = bdyU
         self.backend = backend
+        self.v = float(v)
+        self.coefK_s = np.ascontiguousarray(coefK, dtype=np.float64)
+        # stiffness_update_interval (physicsSolver.py:143-144, 296-324); 0: never
+        self.update_interval = int(update_interval)
+        self.update_counter = 0
+        self.geo = None  # (per-sample stiffness, unit follower load) after an update
         bdy = np.asarray(boundary, dtype=np.int64)
         self.bdyDofs = (3 * bdy[:, None] + np.arange(3)[None, :]).ravel()
         coefK = np.ascontiguousarray(coefK, dtype=np.float64)
@@ -323,7 +378,39 @@ class OracleSolidSolver:
         self.up = self.u - dt * du + 0.5 * (dt ** 2) * ddu
         self.LHS = self.LM + 0.5 * dt * self.LC
 
+    def _geo_update(self):
+        """Stiffness and unit follower load on x + u_n (the reference's update step)."""
+        if self.backend == "reference":
+            S = self.S
+            upd = (self.nodes[None] + self.u.T.reshape(S, self.N, 3)).copy()
+            nnzb = len(self.indices)
+            K = np.zeros((nnzb, S, 3, 3))
+            f = np.zeros((3 * self.N, S))
+            self.ref.OptimizedSolidAssembleUpdate(upd, self.elements, np.array([1.0]),
+                                                  d_matrix(self.v), self.coefK_s, self.indptr,
+                                                  self.indices, K, f)
+            self.geo = ("bsr", K, f)
+        else:
+            Kts, f = geometric_update(self.nodes, self.elements, self.v, self.u)
+            self.geo = ("templates", Kts, f)
+
+    def _kmul_geo(self, u, scale):
+        kind, K, _ = self.geo
+        if kind == "bsr":
+            res = np.zeros_like(u)
+            self.ref.MultiplyByVector(self.indptr, self.indices, scale * K, np.ascontiguousarray(u),
+                                      res)
+            return res
+        N3, S = u.shape
+        ue = u.reshape(-1, 3, S)[self.elements].reshape(self.elements.shape[0], 9, S)
+        ye = np.einsum("seij,ejs->eis", K, ue) * (scale * self.coefK_s)[:, None, :]
+        out = np.zeros((N3 // 3, 3, S))
+        np.add.at(out, self.elements.ravel(), ye.reshape(-1, 3, S))
+        return out.reshape(N3, S)
+
     def _kmul(self, u, scale):
+        if self.geo is not None:
+            return self._kmul_geo(u, scale)
         if self.backend == "reference":
             res = np.zeros_like(u)
             self.ref.MultiplyByVector(self.indptr, self.indices, scale * self.K,
@@ -334,9 +421,22 @@ class OracleSolidSolver:
         return template_multiply(self.elements, self.Kt, scale * self.coefK, u)
 
     def step(self, p):
-        """One ``SolidSolver.Solve`` step (physicsSolver.py:263-292) with pressure ``p``."""
+        """One ``SolidSolver.Solve`` step (physicsSolver.py:263-292) with pressure ``p``.
+
+        With an update interval, the stiffness and the (unit) follower load are rebuilt on
+        x + u_n when the counter reaches the interval (physicsSolver.py:296-324); the load
+        of the step is then ``p`` times the follower load of the last update."""
         dt = self.dt
-        A1 = (dt ** 2) * (p * self.f)[:, None]
+        if self.update_interval:
+            if self.update_counter >= self.update_interval:
+                self._geo_update()
+                self.update_counter = 1
+            else:
+                self.update_counter += 1
+        if self.geo is not None:
+            A1 = (dt ** 2) * p * self.geo[2]
+        else:
+            A1 = (dt ** 2) * (p * self.f)[:, None]
         Ku = self._kmul(self.u, scale=dt ** 2)
         A2 = 2.0 * self.LM * self.u - Ku
         A3 = (0.5 * dt * self.LC - self.LM) * self.up

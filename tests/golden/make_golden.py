@@ -7,7 +7,10 @@ synthetic tubes and stores inputs and outputs in ``tests/golden/*.npz``:
 * ``tube8x6_element.npz``: per-element E and h (coefK = E*h, thickness at the 3
   quadrature points = h), 3 samples, damping 100, linear pressure ramp, 30 steps;
 * ``tube6x5_nodal.npz``: nodal E and h interpolated to the quadrature points as
-  ``physicsSolver.py:146-165`` does, 2 samples, no damping, 20 steps.
+  ``physicsSolver.py:146-165`` does, 2 samples, no damping, 20 steps;
+* ``tube8x6_geo1.npz`` / ``tube8x6_geo3.npz``: as the element tube, with the stiffness
+  and the follower pressure rebuilt on x + u by ``OptimizedSolidAssembleUpdate`` every
+  step / every 3 steps (``stiffness_update_interval``), 30 steps.
 
 Stored: assembled block-CSR K, M, C (reference layout), traction f, lumped LM,
 LC, u_{-1}, and the displacement history every 5 steps.
@@ -26,7 +29,7 @@ from cvfes_b200.mesh import SolidMesh, TubeGeometry, tube_mesh  # noqa: E402
 from oracle.solid_oracle import OracleSolidSolver, load_reference_module  # noqa: E402
 
 
-def run(name, nc, na, S, damp, steps, nodal, seed):
+def run(name, nc, na, S, damp, steps, nodal, seed, update_interval=0):
     rng = np.random.default_rng(seed)
     nodes, elems, inl, outl = tube_mesh(TubeGeometry(nc, na, 3.0, 0.3))
     N, E = len(nodes), len(elems)
@@ -44,7 +47,7 @@ def run(name, nc, na, S, damp, steps, nodal, seed):
     dt = 2e-6
     pres = 1.33e5 * np.minimum(np.arange(steps) / 10.0, 1.0)
     o = OracleSolidSolver(nodes, elems, mesh.boundary, coefK, gthick, 1.0, 0.49, damp, dt,
-                          backend="reference")
+                          backend="reference", update_interval=update_interval)
     up0 = o.up.copy()
     hist = []
     for n, p in enumerate(pres):
@@ -54,7 +57,7 @@ def run(name, nc, na, S, damp, steps, nodal, seed):
     out = dict(nodes=nodes, elements=elems, boundary=mesh.boundary, coefK=coefK, gthick=gthick,
                density=1.0, v=0.49, damp=damp, dt=dt, pressures=pres, indptr=o.indptr,
                indices=o.indices, K=o.K, M=o.M, C=o.C, f=o.f, LM=o.LM, LC=o.LC, up0=up0,
-               hist=np.array(hist))
+               hist=np.array(hist), update_interval=update_interval)
     if nodal:
         out.update(vE=mesh.vE, vthickness=mesh.vthickness)
     np.savez_compressed(os.path.join(HERE, name), **out)
@@ -66,3 +69,5 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref is not built: make -C oracle")
     run("tube8x6_element.npz", 8, 6, 3, 100.0, 30, nodal=False, seed=1)
     run("tube6x5_nodal.npz", 6, 5, 2, 0.0, 20, nodal=True, seed=2)
+    run("tube8x6_geo1.npz", 8, 6, 3, 100.0, 30, nodal=False, seed=1, update_interval=1)
+    run("tube8x6_geo3.npz", 8, 6, 3, 100.0, 30, nodal=False, seed=1, update_interval=3)

@@ -79,3 +79,16 @@ def test_closed_tube_net_pressure_force_is_axial_only():
     # radial components cancel on a closed ring; the open ends leave no axial load either
     assert np.abs(f[:, 0].sum()) < 1e-12 * np.abs(f).sum()
     assert np.abs(f[:, 1].sum()) < 1e-12 * np.abs(f).sum()
+
+
+@pytest.mark.parametrize("name", ["tube8x6_geo1.npz", "tube8x6_geo3.npz"])
+def test_geometric_update_restatement_matches_golden_history(name):
+    """Stiffness and follower pressure rebuilt on x + u (OptimizedSolidAssembleUpdate,
+    pyx:710-819) every 1 / 3 steps: the NumPy restatement against the reference run."""
+    g = dict(np.load(os.path.join(GOLD, name)))
+    o = so.OracleSolidSolver(g["nodes"], g["elements"], g["boundary"], g["coefK"], g["gthick"],
+                             float(g["density"]), float(g["v"]), float(g["damp"]), float(g["dt"]),
+                             backend="numpy", update_interval=int(g["update_interval"]))
+    hist = o.run(g["pressures"], history_every=5)
+    for h, ref in zip(hist, g["hist"]):
+        assert _rel(h, ref) < 1e-12
