@@ -139,6 +139,8 @@ SIGNATURES = {
                                               D, D, D, P, P, P, P]),
     "cvfes_solid_advance_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, I64, P, I32,
                                               D, D, D, P, P, P, P]),
+    "cvfes_solid_stress_f64": (C.c_int, [I64, I64, P, P, P, P, P, D, P, P]),
+    "cvfes_solid_stress_f32": (C.c_int, [I64, I64, P, P, P, P, P, D, P, P]),
     "cvfes_set_adjoint_tuning": (C.c_int, [I32, I32, I32, I32, I32]),
     "cvfes_get_adjoint_tuning": (C.c_int, [I32, P, P, P, P]),
     "cvfes_adjoint_ckpt_count": (C.c_int64, [I64, I64]),

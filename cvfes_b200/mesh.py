@@ -211,6 +211,20 @@ class SolidMesh:
         coefK = np.ascontiguousarray((gH * gE) @ wt)
         return coefK, gH
 
+    def element_moduli(self):
+        """Young's modulus per element and sample (E,S): the mean over the three quadrature
+        points, as the stress recovery uses it (``physicsSolver.py:416-424``).  With only
+        explicit ``coefK``/``gthick`` arrays it is ``coefK`` over the mean thickness."""
+        if self.elmE is not None and self.coefK is None:
+            return np.ascontiguousarray(self.elmE, dtype=np.float64)
+        if self.vE is not None and self.coefK is None:
+            gps = np.array([[0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+            ve = np.asarray(self.vE)[self.elementNodeIds, :].swapaxes(1, 2)
+            return np.ascontiguousarray((ve @ gps.T).mean(axis=2))
+        coefK, gthick = self.element_coefficients()
+        h = gthick.mean(axis=2) if gthick.ndim == 3 else gthick
+        return np.ascontiguousarray(coefK / h)
+
     def UpdateCoordinates(self, u):
         """Deformed coordinates per sample (``mesh.py:678-680``): (S, N, 3)."""
         return (np.tile(self.nodes, (self.nSmp, 1, 1)).reshape(self.nSmp, self.ndof)

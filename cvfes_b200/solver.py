@@ -459,13 +459,36 @@ class GPUSolidSolver(PhysicsSolver):
         resU[self.dofs, :] = quant
         return resU
 
+    def Stress(self) -> torch.Tensor:
+        """Element stresses (E, S, 5: xx, yy, xy, xz, yz) of the current state on the
+        geometry of the last stiffness update (``physicsSolver.py:416-424``)."""
+        dev = self.device
+        with torch.cuda.device(dev):
+            if getattr(self, "_young", None) is None:
+                self._young = torch.from_numpy(self.mesh.element_moduli()).to(dev)
+            dtype = torch.float64 if self.precision == 64 else torch.float32
+            out = torch.empty((self.nElms, self.nSmp, 5), dtype=dtype, device=dev)
+            ug = None
+            if self.update_interval > 0 and self.geo_counter > 0:
+                # the geometry of the last update: u at the start of the last step when it
+                # is refreshed every step, else the copy taken at the update
+                ug = self.bufs[self.prev] if self.geo_live else self.ugeo
+            fn = "cvfes_solid_stress_f64" if self.precision == 64 else "cvfes_solid_stress_f32"
+            call(fn, self.nElms, self.nSmp, ptr(self.plan.nodes), ptr(self.plan.elems),
+                 ptr(self._young), ptr(self.bufs[self.cur]), ptr(ug), float(self.mesh.v),
+                 ptr(out), self._stream())
+        return out
+
     def Save(self, filename, counter):
-        """Displacement of every sample at this step (``physicsSolverSDampGPUs.py:452-464``)."""
+        """Displacement and element stresses of every sample at this step
+        (``physicsSolver.py:383-397``; ``physicsSolverSDampGPUs.py:452-464``)."""
         resU = self.displacement()
+        stress = self.Stress().double().cpu().numpy()
         if self.rank == 0:
             from .io import save_displacement
             save_displacement(filename, counter, self.mesh,
-                              resU.T.reshape(self.nSmp, self.mesh.nNodes, self.Dof))
+                              resU.T.reshape(self.nSmp, self.mesh.nNodes, self.Dof),
+                              stress=stress)
         self.comm.Barrier()
 
 

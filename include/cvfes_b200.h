@@ -344,6 +344,20 @@ int cvfes_solid_advance_geo_f32(const cvfes_solid_mesh* mesh, const float* coef,
                                 double damp, int32_t* cur_idx, int32_t* prev_idx,
                                 int32_t* geo_live_out, void* stream);
 
+/* ------------------------------------------------------------ stress recovery
+ * Element stresses per sample (OptimizedCalculateStress, optimizedSolidAssemble.pyx:
+ * 1116-1223; physicsSolver.py:416-424 at each save): global xx, yy, xy, xz, yz of
+ * T^T (E D B TT u_e) T on the geometry x + u_g.
+ *   nodes device f64 [N][3], elems device int32 [E][3] (the state's node numbering),
+ *   young device f64 [E][S] (mean of E over the quadrature points), u [3N][S],
+ *   ug [3N][S] geometry displacement or NULL (undeformed), stress out [E][S][5].   */
+int cvfes_solid_stress_f64(int64_t n_elems, int64_t n_samples, const double* nodes,
+                           const int32_t* elems, const double* young, const double* u,
+                           const double* ug, double nu, double* stress, void* stream);
+int cvfes_solid_stress_f32(int64_t n_elems, int64_t n_samples, const double* nodes,
+                           const int32_t* elems, const double* young, const float* u,
+                           const float* ug, double nu, float* stress, void* stream);
+
 /* ------------------------------------------------------------ adjoint
  * Gradient of the displacement-mismatch objective
  *     J_s = sum_{n % obs_every == 0, 0 < n <= T} sum_{i in obs} |u_n(i) - uobs_n(i)|^2

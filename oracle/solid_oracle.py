@@ -228,16 +228,10 @@ def template_multiply(elements, Kt, coefK, u):
     return out.reshape(N3, S)
 
 
-def geometric_update(nodes, elements, v, u):
-    """Restatement of ``OptimizedSolidAssembleUpdate`` (pyx:710-819) with unit traction, per
-    sample on the coordinates ``x + u_s`` (``mesh.py:678-680``): the unit stiffness of every
-    element per sample (S,E,9,9) and the unit follower load (3N, S).  Same steps as
-    ``element_frames`` / ``element_templates``, batched over samples."""
-    N = nodes.shape[0]
-    S = u.shape[1]
-    E = elements.shape[0]
-    xs = nodes[None] + u.T.reshape(S, N, 3)
-    p = xs[:, elements]                                   # (S,E,3,3): sample, elem, node, xyz
+def batched_frames(p):
+    """``element_frames`` for coordinates ``p`` (S,E,3,3) of every sample: T (S,E,3,3),
+    area (S,E) and B (S,E,5,9) (pyx:82-127, 530-560)."""
+    S, E = p.shape[:2]
     e0 = p[:, :, 2] - p[:, :, 1]
     e1 = p[:, :, 0] - p[:, :, 2]
     T = np.empty((S, E, 3, 3))
@@ -264,17 +258,56 @@ def geometric_update(nodes, elements, v, u):
                         (1, 4): x13, (2, 3): x13, (4, 5): x13,
                         (1, 7): x21, (2, 6): x21, (4, 8): x21}.items():
         B[:, :, r, c] = val / c1
-    Bt = np.swapaxes(B, -1, -2)
-    btdb = (Bt @ d_matrix(v)) @ B * area[..., None, None]
+    return T, area, B
+
+
+def _block_rot(T):
+    S, E = T.shape[:2]
     TT = np.zeros((S, E, 9, 9))
     for a in range(3):
         TT[:, :, 3 * a:3 * a + 3, 3 * a:3 * a + 3] = T
+    return TT
+
+
+def geometric_update(nodes, elements, v, u):
+    """Restatement of ``OptimizedSolidAssembleUpdate`` (pyx:710-819) with unit traction, per
+    sample on the coordinates ``x + u_s`` (``mesh.py:678-680``): the unit stiffness of every
+    element per sample (S,E,9,9) and the unit follower load (3N, S)."""
+    N = nodes.shape[0]
+    S = u.shape[1]
+    xs = nodes[None] + u.T.reshape(S, N, 3)
+    T, area, B = batched_frames(xs[:, elements])
+    Bt = np.swapaxes(B, -1, -2)
+    btdb = (Bt @ d_matrix(v)) @ B * area[..., None, None]
+    TT = _block_rot(T)
     Kt = np.swapaxes(TT, -1, -2) @ btdb @ TT
     f = np.zeros((N, 3, S))
     load = (area / 3.0)[..., None] * T[:, :, 2]           # (S,E,3)
     for a in range(3):
         np.add.at(f, elements[:, a], load.transpose(1, 2, 0))
     return Kt, f.reshape(3 * N, S)
+
+
+def calculate_stress(nodes_s, elements, v, young, u):
+    """Restatement of ``OptimizedCalculateStress`` (pyx:1116-1223): on the per-sample
+    coordinates ``nodes_s`` (S,N,3), the global (xx, yy, xy, xz, yz) entries of
+    ``T^T (E D B TT u_e) T`` per element and sample, (E,S,5)."""
+    S, N = nodes_s.shape[:2]
+    T, area, B = batched_frames(nodes_s[:, elements])
+    TT = _block_rot(T)
+    ue = u.reshape(N, 3, S)[elements].reshape(elements.shape[0], 9, S).transpose(2, 0, 1)
+    lU = np.einsum("seij,sej->sei", TT, ue)
+    ls = np.einsum("kl,selj,sej->sek", d_matrix(v), B, lU) * young.T[..., None]
+    L = np.zeros(T.shape)
+    L[..., 0, 0] = ls[..., 0]
+    L[..., 0, 1] = L[..., 1, 0] = ls[..., 2]
+    L[..., 0, 2] = L[..., 2, 0] = ls[..., 3]
+    L[..., 1, 1] = ls[..., 1]
+    L[..., 1, 2] = L[..., 2, 1] = ls[..., 4]
+    G = np.swapaxes(T, -1, -2) @ L @ T
+    out = np.stack([G[..., 0, 0], G[..., 1, 1], G[..., 0, 1], G[..., 0, 2], G[..., 1, 2]],
+                   axis=-1)
+    return out.transpose(1, 0, 2).copy()
 
 
 # --------------------------------------------------------------------------------------
@@ -318,6 +351,7 @@ class OracleSolidSolver:
         self.update_interval = int(update_interval)
         self.update_counter = 0
         self.geo = None  # (per-sample stiffness, unit follower load) after an update
+        self.update_nodes = None  # x + u at the last update, (S, N, 3)
         bdy = np.asarray(boundary, dtype=np.int64)
         self.bdyDofs = (3 * bdy[:, None] + np.arange(3)[None, :]).ravel()
         coefK = np.ascontiguousarray(coefK, dtype=np.float64)
@@ -380,6 +414,7 @@ class OracleSolidSolver:
 
     def _geo_update(self):
         """Stiffness and unit follower load on x + u_n (the reference's update step)."""
+        self.update_nodes = (self.nodes[None] + self.u.T.reshape(self.S, self.N, 3)).copy()
         if self.backend == "reference":
             S = self.S
             upd = (self.nodes[None] + self.u.T.reshape(S, self.N, 3)).copy()
@@ -446,6 +481,19 @@ class OracleSolidSolver:
         self.up = self.u
         self.u = u
         return u
+
+    def stress(self, young):
+        """Element stresses (E,S,5) of the current state on the geometry of the last update
+        (``physicsSolver.py:416-424``); ``young`` (E,S) is the mean E of each element."""
+        nodes_s = self.update_nodes if self.update_nodes is not None else \
+            np.repeat(self.nodes[None], self.S, axis=0)
+        if self.backend == "reference":
+            out = np.empty((self.elements.shape[0], self.S, 5))
+            self.ref.OptimizedCalculateStress(np.ascontiguousarray(nodes_s), self.elements,
+                                              d_matrix(self.v), np.ascontiguousarray(young),
+                                              np.ascontiguousarray(self.u), out)
+            return out
+        return calculate_stress(nodes_s, self.elements, self.v, young, self.u)
 
     def run(self, pressures, history_every=0):
         hist = []

@@ -13,7 +13,8 @@ synthetic tubes and stores inputs and outputs in ``tests/golden/*.npz``:
   step / every 3 steps (``stiffness_update_interval``), 30 steps.
 
 Stored: assembled block-CSR K, M, C (reference layout), traction f, lumped LM,
-LC, u_{-1}, and the displacement history every 5 steps.
+LC, u_{-1}, the displacement history every 5 steps and the element stresses of the
+final state (``OptimizedCalculateStress``, with E the per-element mean modulus).
 
     make -C oracle && python tests/golden/make_golden.py
 """
@@ -54,7 +55,10 @@ def run(name, nc, na, S, damp, steps, nodal, seed, update_interval=0):
         o.step(p)
         if (n + 1) % 5 == 0:
             hist.append(o.u.copy())
+    young = mesh.element_moduli()
+    stress = o.stress(young)
     out = dict(nodes=nodes, elements=elems, boundary=mesh.boundary, coefK=coefK, gthick=gthick,
+               young=young, stress=stress,
                density=1.0, v=0.49, damp=damp, dt=dt, pressures=pres, indptr=o.indptr,
                indices=o.indices, K=o.K, M=o.M, C=o.C, f=o.f, LM=o.LM, LC=o.LC, up0=up0,
                hist=np.array(hist), update_interval=update_interval)

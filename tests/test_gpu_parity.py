@@ -342,3 +342,30 @@ def test_geometric_update_large_samples_against_oracle(lib, cuda):
         s = GPUSolidSolver(LocalComm(), mesh, cfg)
         s.Advance(pres)
         assert so.rel_l2(s.displacement(), o.u) < tol
+
+
+@pytest.mark.parametrize("name", ["tube8x6_element.npz", "tube6x5_nodal.npz",
+                                  "tube8x6_geo1.npz", "tube8x6_geo3.npz"])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_stress_recovery_matches_golden(lib, cuda, name, precision, tmp_path):
+    """GPUSolidSolver.Stress after the golden run against the reference's
+    OptimizedCalculateStress; Save writes the same stresses next to the displacement."""
+    g = golden(name)
+    mesh = golden_mesh(g)
+    if "vE" in g:
+        mesh = SolidMesh(g["nodes"], g["elements"], g["boundary"], g["coefK"].shape[1],
+                         density=float(g["density"]), v=float(g["v"]), damp=float(g["damp"]),
+                         vE=g["vE"], vthickness=g["vthickness"])
+    cfg = Cfg(float(g["dt"]), mesh.nSmp, precision)
+    cfg.update_interval = int(g["update_interval"])
+    solver = GPUSolidSolver(LocalComm(), mesh, cfg)
+    for p in g["pressures"]:
+        solver.pressure = float(p)
+        solver.Solve(None, float(g["dt"]))
+    st = solver.Stress().double().cpu().numpy()
+    tol = 1e-12 if precision == 64 else 1e-4
+    assert rel(st, g["stress"]) < tol
+    solver.Save(str(tmp_path / "out.npz"), 7)
+    saved = np.load(str(tmp_path / "out7.npz"))
+    assert np.array_equal(saved["stress"], st)
+    assert saved["u"].shape == (mesh.nSmp, mesh.nNodes, 3)

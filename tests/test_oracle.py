@@ -92,3 +92,16 @@ def test_geometric_update_restatement_matches_golden_history(name):
     hist = o.run(g["pressures"], history_every=5)
     for h, ref in zip(hist, g["hist"]):
         assert _rel(h, ref) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["tube8x6_element.npz", "tube6x5_nodal.npz",
+                                  "tube8x6_geo1.npz", "tube8x6_geo3.npz"])
+def test_stress_restatement_matches_golden(name):
+    """Element stresses (OptimizedCalculateStress, pyx:1116-1223) of the final state, on the
+    undeformed geometry or on the geometry of the last update."""
+    g = dict(np.load(os.path.join(GOLD, name)))
+    o = so.OracleSolidSolver(g["nodes"], g["elements"], g["boundary"], g["coefK"], g["gthick"],
+                             float(g["density"]), float(g["v"]), float(g["damp"]), float(g["dt"]),
+                             backend="numpy", update_interval=int(g["update_interval"]))
+    o.run(g["pressures"])
+    assert _rel(o.stress(g["young"]), g["stress"]) < 1e-12
