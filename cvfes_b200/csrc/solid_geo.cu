@@ -10,7 +10,8 @@
 // slot's reference edge vectors X_b - X_a (exact, precomputed) plus the neighbour
 // displacement differences, so the FP32 form never subtracts large coordinates.
 // Per slot and sample: the local frame (x along edge 1->2, y the Gram-Schmidt of
-// edge 2->0, z = x cross y), the in-plane coordinates, the area, the 3x3 local blocks
+// edge 2->0, z = x cross y; unit vectors by rsqrt), the in-plane coordinates, the
+// area, the 3x3 local blocks
 // of B^T D B (membrane + transverse shear, D / (1 - nu^2)) of row a against its two
 // neighbours applied to the neighbours' displacement differences in the local frame,
 // and the result rotated back; rigid translations are in the null space, so the row
@@ -56,6 +57,7 @@ struct GeoConst {
     T pe1;  // (1 - nu) / 2
     T pe2;  // k (1 - nu) / 2
     T pe3;  // 1 - nu^2
+    T inv4pe3;  // 1 / (4 (1 - nu^2))
 };
 
 template <typename T>
@@ -86,17 +88,17 @@ __device__ __forceinline__ void geo_row(int la, const T (&q1)[3], const T (&q2)[
     T ex[3], ey[3], ez[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ex[d] = P[2][d] - P[1][d];
-    T nrm = sqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
+    T inv = rsqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) ex[d] = ex[d] / nrm;
+    for (int d = 0; d < 3; ++d) ex[d] *= inv;
 #pragma unroll
     for (int d = 0; d < 3; ++d) ey[d] = P[0][d] - P[2][d];
     const T pr = ex[0] * ey[0] + ex[1] * ey[1] + ex[2] * ey[2];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ey[d] -= pr * ex[d];
-    nrm = sqrt(ey[0] * ey[0] + ey[1] * ey[1] + ey[2] * ey[2]);
+    inv = rsqrt(ey[0] * ey[0] + ey[1] * ey[1] + ey[2] * ey[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) ey[d] = ey[d] / nrm;
+    for (int d = 0; d < 3; ++d) ey[d] *= inv;
     ez[0] = ex[1] * ey[2] - ex[2] * ey[1];
     ez[1] = ex[2] * ey[0] - ex[0] * ey[2];
     ez[2] = ex[0] * ey[1] - ex[1] * ey[0];
@@ -137,11 +139,12 @@ __device__ __forceinline__ void geo_row(int la, const T (&q1)[3], const T (&q2)[
         r[1] += (cb * K.pe0 + bc * K.pe1) * w2[0] + (cc + bb * K.pe1) * w2[1];
         r[2] += (bb + cc) * K.pe2 * w2[2];
     }
-    const T scale = c / (T(4) * area * K.pe3);
+    const T scale = c * K.inv4pe3 / area;
+    const T a3 = area * T(1.0 / 3.0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         acc[d] += scale * (r[0] * ex[d] + r[1] * ey[d] + r[2] * ez[d]);
-        load[d] += area / T(3) * ez[d];
+        load[d] += a3 * ez[d];
     }
 }
 
@@ -274,6 +277,7 @@ int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, con
     G.K.pe1 = (T)(0.5 * (1.0 - nu));
     G.K.pe2 = (T)(0.5 * shear_k * (1.0 - nu));
     G.K.pe3 = (T)(1.0 - nu * nu);
+    G.K.inv4pe3 = (T)(0.25 / (1.0 - nu * nu));
     const bool same = G.ug == u;
     const void* ptrs[6] = {coef, invm, u, up, un, G.ug};
     int V = (int)(16 / sizeof(T));

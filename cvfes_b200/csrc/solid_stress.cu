@@ -39,17 +39,17 @@ __global__ void k_stress(long long n_elems, int S, const double* __restrict__ no
     T ex[3], ey[3], ez[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ex[d] = P[2][d] - P[1][d];
-    T nrm = sqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
+    T inv = rsqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) ex[d] = ex[d] / nrm;
+    for (int d = 0; d < 3; ++d) ex[d] *= inv;
 #pragma unroll
     for (int d = 0; d < 3; ++d) ey[d] = P[0][d] - P[2][d];
     const T pr = ex[0] * ey[0] + ex[1] * ey[1] + ex[2] * ey[2];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ey[d] -= pr * ex[d];
-    nrm = sqrt(ey[0] * ey[0] + ey[1] * ey[1] + ey[2] * ey[2]);
+    inv = rsqrt(ey[0] * ey[0] + ey[1] * ey[1] + ey[2] * ey[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) ey[d] = ey[d] / nrm;
+    for (int d = 0; d < 3; ++d) ey[d] *= inv;
     ez[0] = ex[1] * ey[2] - ex[2] * ey[1];
     ez[1] = ex[2] * ey[0] - ex[0] * ey[2];
     ez[2] = ex[0] * ey[1] - ex[1] * ey[0];

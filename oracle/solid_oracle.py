@@ -455,7 +455,7 @@ class OracleSolidSolver:
             return multiply_by_vector(self.indptr, self.indices, scale * self.K, u)
         return template_multiply(self.elements, self.Kt, scale * self.coefK, u)
 
-    def step(self, p):
+    def step(self, p, trac=None):
         """One ``SolidSolver.Solve`` step (physicsSolver.py:263-292) with pressure ``p``.
 
         With an update interval, the stiffness and the (unit) follower load are rebuilt on
@@ -472,6 +472,9 @@ class OracleSolidSolver:
             A1 = (dt ** 2) * p * self.geo[2]
         else:
             A1 = (dt ** 2) * (p * self.f)[:, None]
+        if trac is not None:
+            # nodal traction of the GPU path (calc_u_appTrac, physicsSolverSDampGPUs.cl:436-446)
+            A1 = A1 + (dt ** 2) * np.asarray(trac, dtype=np.float64).reshape(-1)[:, None]
         Ku = self._kmul(self.u, scale=dt ** 2)
         A2 = 2.0 * self.LM * self.u - Ku
         A3 = (0.5 * dt * self.LC - self.LM) * self.up

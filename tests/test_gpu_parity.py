@@ -369,3 +369,55 @@ def test_stress_recovery_matches_golden(lib, cuda, name, precision, tmp_path):
     saved = np.load(str(tmp_path / "out7.npz"))
     assert np.array_equal(saved["stress"], st)
     assert saved["u"].shape == (mesh.nSmp, mesh.nNodes, 3)
+
+
+@pytest.mark.parametrize("constant", [False, True])
+def test_traction_series_input_against_oracle(lib, cuda, tmp_path, constant):
+    """Fluid wall traction read from the .npy series of RefreshContext (ramped, then
+    interpolated between files every dt_f; or one constant file), added as nodal force."""
+    import math
+    g = golden("tube8x6_element.npz")
+    mesh = golden_mesh(g)
+    N, dt = mesh.nNodes, float(g["dt"])
+    rng = np.random.default_rng(9)
+    base = str(tmp_path / "trac")
+    files = [2e3 * rng.standard_normal((N, 3)) for _ in range(6)]
+    if constant:
+        np.save(base + ".npy", files[0])
+    else:
+        for i, f in enumerate(files):
+            np.save(f"{base}{i}.npy", f)
+    cfg = Cfg(dt, mesh.nSmp, 64)
+    cfg.exportBdyStressFilename = base
+    cfg.useConstantStress = constant
+    cfg.constant_T, cfg.dt_f, cfg.constant_pressure = 10 * dt, 4 * dt, 5e4
+    solver = GPUSolidSolver(LocalComm(), mesh, cfg)
+    coefK, gthick = mesh.element_coefficients()
+    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
+                             mesh.density, mesh.v, mesh.damp, dt, backend="numpy")
+    bdy = (3 * np.asarray(mesh.boundary)[:, None] + np.arange(3)).ravel()
+
+    class Clock:
+        t = 0.0
+    clock = Clock()
+    T, dtf = cfg.constant_T, cfg.dt_f
+    strac, etrac, nt = files[0], files[1], 0
+    for n in range(30):
+        clock.t = t = n * dt
+        solver.RefreshContext(clock)
+        solver.Solve(t, dt)
+        # expected load (physicsSolverSDampGPUs.py:287-322), boundary rows held clamped
+        if constant:
+            tr = files[0] if t > T else files[0] / 2 - files[0] / 2 * math.cos(math.pi / T * t)
+        elif t > T:
+            if int((t - T) / dtf) > nt:
+                nt += 1
+                strac, etrac = etrac, files[nt + 1]
+            tr = strac + (t - T - nt * dtf) * (etrac - strac) / dtf
+        else:
+            tr = strac / 2 - strac / 2 * math.cos(math.pi / T * t)
+        tr = np.array(tr, dtype=np.float64).reshape(-1)
+        tr[bdy] = 0.0
+        p = 5e4 if t > T else 5e4 * t / T  # the configuration's linear ramp
+        o.step(p, tr)
+    assert so.rel_l2(solver.displacement(), o.u) < FP64_TOL
