@@ -512,8 +512,10 @@ def run_batched(args):
             "config": {"workload": "batched64", "tubes": len(cases),
                        "nodes": sum(m.nNodes for m in meshes),
                        "elements": sum(m.nElements for m in meshes), "samples": S_total,
-                       "parallelism": f"replicas{world}", "tuning": tuned.get("vec"),
-                       "grid": tuned.get("grid"), "l2": "state > L2, no flush",
+                       "parallelism": f"replicas{world}", "kernel": ("fan" if batch.variant == 1
+                                                                    else "row gather"),
+                       "vec": tuned.get("vec"), "grid": tuned.get("grid"),
+                       "l2": "state > L2, no flush",
                        "finite": finite},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],

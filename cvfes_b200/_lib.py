@@ -126,11 +126,11 @@ SIGNATURES = {
     "cvfes_get_step_tuning": (C.c_int, [I32, P, P, P, P]),
     "cvfes_status_read": (C.c_int, [P, P]),
     "cvfes_batch_table_bytes": (C.c_int64, [I32]),
-    "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, C.POINTER(C.c_int64)]),
-    "cvfes_batch_step": (C.c_int, [P, I32, I64, I32, I32, I32, P, I64, I32, P]),
-    "cvfes_batch_advance": (C.c_int, [P, I32, I64, I32, I32, I32, P, I64, I32,
+    "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, P]),
+    "cvfes_batch_step": (C.c_int, [P, I32, P, I32, I32, I32, I32, P, I64, I32, P]),
+    "cvfes_batch_advance": (C.c_int, [P, I32, P, I32, I32, I32, I32, P, I64, I32,
                                       C.POINTER(C.c_int32), P]),
-    "cvfes_batch_graph_capture": (C.c_int, [P, I32, I64, I32, I32, P, I64, I32,
+    "cvfes_batch_graph_capture": (C.c_int, [P, I32, P, I32, I32, I32, P, I64, I32,
                                             C.POINTER(C.c_void_p)]),
     "cvfes_solid_slot_geometry_f64": (C.c_int, [I64, P, P, P, P, P, P]),
     "cvfes_solid_step_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),

@@ -4,8 +4,10 @@ Each mesh keeps its own ``GPUSolidSolver`` (plan, material, three state buffers,
 start-up state), so its sample count, time step and damping are its own.  The
 batch packs one descriptor per mesh into a device table and advances all meshes
 with one persistent kernel launch per step (``cvfes_batch_step``), captured in CUDA
-graphs of ``graph_chunk`` steps.  A mesh advanced in a batch is bitwise identical
-to the same mesh advanced alone by the L1 single-mesh kernel.
+graphs of ``graph_chunk`` steps.  Two kernels: the fan kernel (``variant`` 1, the
+default: slot rows staged by TMA, fan-rotation gathers) and the row-gather kernel
+(``variant`` 0).  A mesh advanced in a batch is bitwise identical to the same mesh
+advanced alone by the single-mesh kernels.
 """
 from __future__ import annotations
 
@@ -37,7 +39,7 @@ class BatchedSolidSolver:
 
     def __init__(self, meshes: Sequence, dts: Sequence[float], precision: int = 32,
                  device="cuda:0", vec: Optional[int] = None, grid: int = 0,
-                 graph_chunk: int = 48, max_steps: int = 8192):
+                 graph_chunk: int = 48, max_steps: int = 8192, variant: int = 1):
         if len(meshes) != len(dts) or not meshes:
             raise ValueError("one dt per mesh")
         if graph_chunk % 3:
@@ -56,6 +58,8 @@ class BatchedSolidSolver:
                 vec //= 2
         self.vec = vec
         self.grid = grid
+        self.variant = variant
+        self.totals = (_lib.C.c_int64 * 3)()
         self.graph_chunk = graph_chunk
         self.rot = 0
         self.steps = 0
@@ -80,16 +84,25 @@ class BatchedSolidSolver:
             it.p_sched = ptr(self._p)
             it.dt = self.dts[i]
             it.damp = float(s.damp)
-        total = _lib.C.c_int64()
         with torch.cuda.device(self.device):
             call("cvfes_batch_pack", items, n, self.precision, self.vec, ptr(self.table),
-                 _lib.C.byref(total))
-        self.total_items = int(total.value)
+                 self.totals)
+        if self.variant == 1 and self.totals[2] <= 0:
+            self.variant = 0  # a mesh without max_degree: the fan stage cannot be sized
+        self.total_items = int(self.totals[self.variant])
         self.n_meshes = n
         self.release_graphs()
 
-    def set_launch(self, vec: Optional[int] = None, grid: Optional[int] = None):
-        """Change the tile shape (samples per thread) or the persistent grid size."""
+    def set_launch(self, vec: Optional[int] = None, grid: Optional[int] = None,
+                   variant: Optional[int] = None):
+        """Change the tile shape (samples per thread), the persistent grid size or the
+        kernel (0 row gather, 1 fan)."""
+        if variant is not None and variant != self.variant:
+            if variant == 1 and self.totals[2] <= 0:
+                raise ValueError("the fan kernel needs every mesh's max_degree")
+            self.variant = variant
+            self.total_items = int(self.totals[variant])
+            self.release_graphs()
         if vec is not None and vec != self.vec:
             self.vec = vec
             self._pack()
@@ -103,8 +116,8 @@ class BatchedSolidSolver:
     # ------------------------------------------------------------------ stepping
     def _plain(self, n):
         rot_out = _lib.C.c_int32()
-        call("cvfes_batch_advance", ptr(self.table), self.n_meshes, self.total_items,
-             self.precision, self.vec, self.rot, ptr(self.clock), n, self.grid,
+        call("cvfes_batch_advance", ptr(self.table), self.n_meshes, self.totals,
+             self.precision, self.vec, self.variant, self.rot, ptr(self.clock), n, self.grid,
              _lib.C.byref(rot_out), self._stream())
         self.rot = rot_out.value
 
@@ -139,12 +152,13 @@ class BatchedSolidSolver:
         return self
 
     def _graph(self, chunk):
-        key = (chunk, self.vec, self.grid)
+        key = (chunk, self.vec, self.grid, self.variant)
         g = self._graphs.get(key)
         if g is None:
             h = _lib.C.c_void_p()
-            call("cvfes_batch_graph_capture", ptr(self.table), self.n_meshes, self.total_items,
-                 self.precision, self.vec, ptr(self.clock), chunk, self.grid, _lib.C.byref(h))
+            call("cvfes_batch_graph_capture", ptr(self.table), self.n_meshes, self.totals,
+                 self.precision, self.vec, self.variant, ptr(self.clock), chunk, self.grid,
+                 _lib.C.byref(h))
             g = self._graphs[key] = h.value
         return g
 

@@ -266,113 +266,6 @@ __global__ void k_bsr_spmv(long long n_nodes, int S, const long long* __restrict
 __global__ void k_clock_add(long long* clock, long long n) { clock[0] += n; }
 
 // ------------------------------------------------------------ fan-rotation step
-// The fan order makes the first neighbour of element k the second neighbour of
-// element k-1, so element k needs only one new neighbour row set.  Three register
-// buffers rotate through the roles (previous = first neighbour, current = second
-// neighbour, next = in flight); the slot loop is unrolled three times so the
-// rotation is a renaming, not a copy.  Neighbour rows are turned into differences
-// u_b - u_a once (FP32 form) and reused by the following element.
-template <typename T, int V>
-__device__ __forceinline__ void load_rows(Vec<T, V> (&x)[3], const T* __restrict__ u, int node,
-                                          size_t S, size_t col) {
-    const T* p = u + (size_t)node * 3 * S + col;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) x[d] = ldg<T, V>(p + d * S);
-}
-template <typename T, int V, bool DIFF>
-__device__ __forceinline__ void to_diff(Vec<T, V> (&x)[3], const Vec<T, V> (&ua)[3]) {
-    if constexpr (DIFF) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) x[d] = vsub(x[d], ua[d]);
-    }
-}
-template <typename T, int V, bool DIFF>
-__device__ __forceinline__ void slot_fma(const T* K, const Vec<T, V>& c, const Vec<T, V> (&d1)[3],
-                                         const Vec<T, V> (&d2)[3], const Vec<T, V> (&ua)[3],
-                                         Vec<T, V> (&acc)[3]) {
-    T kk[28];
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int q = (DIFF ? 2 : 0); q < 7; ++q) {
-            const float4 t = reinterpret_cast<const float4*>(K)[q];
-            kk[4 * q] = t.x;
-            kk[4 * q + 1] = t.y;
-            kk[4 * q + 2] = t.z;
-            kk[4 * q + 3] = t.w;
-        }
-    } else {
-#pragma unroll
-        for (int q = (DIFF ? 4 : 0); q < 14; ++q) {
-            const double2 t = reinterpret_cast<const double2*>(K)[q];
-            kk[2 * q] = t.x;
-            kk[2 * q + 1] = t.y;
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        Vec<T, V> t = vzero<T, V>();
-        if constexpr (!DIFF) {
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
-        }
-#pragma unroll
-        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], d1[jj]);
-#pragma unroll
-        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], d2[jj]);
-        vfma(acc[i], c, t);
-    }
-}
-
-// One element of the fan: prev holds the first neighbour (difference), cur the
-// second one as loaded; the next element's row set is issued into nxt first.
-template <typename T, int V, bool DIFF>
-__device__ __forceinline__ void fan_phase(int& k, int k1, const int4* srec, const T* sslab,
-                                          const T* __restrict__ u, const T* __restrict__ coef,
-                                          size_t S, size_t col, const Vec<T, V> (&ua)[3],
-                                          Vec<T, V> (&acc)[3], Vec<T, V> (&prev)[3],
-                                          Vec<T, V> (&cur)[3], const Vec<T, V>& ccur,
-                                          Vec<T, V> (&nxt)[3], Vec<T, V>& cnxt) {
-    const bool more = k + 1 < k1;
-    int4 rn = make_int4(0, 0, 0, 1);
-    if (more) {
-        rn = srec[k + 1];
-        load_rows<T, V>(nxt, u, rn.z, S, col);
-        cnxt = ldg<T, V>(coef + (size_t)rn.x * S + col);
-    }
-    to_diff<T, V, DIFF>(cur, ua);
-    slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, prev, cur, ua, acc);
-    if (more && !(rn.w & 1)) {  // fan break: the next element's first neighbour is new
-        load_rows<T, V>(cur, u, rn.y, S, col);
-        to_diff<T, V, DIFF>(cur, ua);
-    }
-    ++k;
-}
-
-template <typename T, int V, bool DIFF>
-__device__ __forceinline__ void ku_row_fan(const int4* srec, const T* sslab, int k0, int k1,
-                                           const T* __restrict__ u, const T* __restrict__ coef,
-                                           size_t S, size_t col, const Vec<T, V> (&ua)[3],
-                                           Vec<T, V> (&acc)[3]) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
-    if (k0 >= k1) return;
-    Vec<T, V> B0[3], B1[3], B2[3], c0, c1, c2;
-    const int4 r0 = srec[k0];
-    load_rows<T, V>(B0, u, r0.y, S, col);
-    load_rows<T, V>(B1, u, r0.z, S, col);
-    c1 = ldg<T, V>(coef + (size_t)r0.x * S + col);
-    to_diff<T, V, DIFF>(B0, ua);
-    int k = k0;
-    while (true) {
-        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B0, B1, c1, B2, c2);
-        if (k >= k1) break;
-        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B1, B2, c2, B0, c0);
-        if (k >= k1) break;
-        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B2, B0, c0, B1, c1);
-        if (k >= k1) break;
-    }
-}
-
 // TMA-staged slot rows (as k_step_staged) + the fan-rotation row; 1D grid with the
 // sample chunk fastest, so the chunks of one node block share its slot rows in L2.
 template <typename T, int V, bool DIFF, int MINB>
@@ -436,6 +329,100 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
     ku_row_fan<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
     step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+}
+
+// ------------------------------------------------------------ persistent fan step
+// The fan kernel as a persistent grid: each block walks work items (node block, sample
+// chunk; chunk fastest) with a stride of the grid, and stages the slot records and
+// stiffness rows of its NEXT item by TMA into the other of two shared-memory stages
+// while the warps multiply the current one, so the per-item staging latency is off the
+// critical path.  Stage s of the block's i-th item completes its mbarrier's phase
+// (i / 2) % 2; a block barrier at the end of every item frees the stage for reuse.
+template <typename T>
+__device__ __forceinline__ void fanp_issue(const StepArgs<T>& A, long long w, uint32_t bar,
+                                           int4* srec, T* sslab) {
+    const long long nb = w / A.nch;
+    const long long a0 = nb * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots || nsl <= 0) {
+        if (nsl > A.cap_slots && A.status) atomicOr(A.status, 2);
+        mbar_arrive_expect_tx(bar, 0);
+        return;
+    }
+    const uint32_t b_rec = (uint32_t)nsl * 16u;
+    const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+    mbar_arrive_expect_tx(bar, b_rec + b_slab);
+    bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+    bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+}
+
+template <typename T, int V, bool DIFF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long long n_items) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const size_t stage_bytes = (size_t)A.cap_slots * (16 + kSlabStride * sizeof(T));
+    // stage q: barrier at smem + 8q, records then stiffness rows at smem + 16 + q * stage_bytes
+    const uint32_t bar0 = smem_u32(smem);
+    int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
+    T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+    }
+    __syncthreads();
+    long long w = blockIdx.x;
+    if (threadIdx.x == 0 && w < n_items) fanp_issue<T>(A, w, bar0, srec0, sslab0);
+    const size_t S = (size_t)A.S;
+    const T p = step_pressure<T>(A);
+    for (int it = 0; w < n_items; w += gridDim.x, ++it) {
+        const int sg = it & 1;
+        const long long wn = w + gridDim.x;
+        if (threadIdx.x == 0 && wn < n_items)
+            fanp_issue<T>(A, wn, bar0 + 8 * (sg ^ 1), stage_rec(srec0, stage_bytes, sg ^ 1), stage_slab(sslab0, stage_bytes, sg ^ 1));
+        const long long nb = w / A.nch;
+        const int chunk = (int)(w - nb * A.nch);
+        const long long a0 = nb * A.npb;
+        const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+        const long long a = a0 + warp;
+        const bool active = warp < A.npb && a < a1;
+        const size_t col = ((size_t)chunk * 32 + lane) * V;
+        const size_t row = (size_t)a * 3 * S + col;
+        const bool clamped = a < A.n_clamped;
+        Vec<T, V> ua[3];
+        T f[3];
+        if (active && !clamped) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ua[d] = ldg<T, V>(A.u + row + d * S);
+                prefetch_l2(A.up + row + d * S);
+            }
+            prefetch_l2(A.invm + (size_t)a * S + col);
+            node_load<T>(A, a, p, f);
+        }
+        if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
+            if (lane == 0 && A.status) atomicOr(A.status, 1);
+            return;
+        }
+        if (active) {
+            if (clamped) {
+                const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+            } else {
+                const int kb = __ldg(A.node_ptr + a0);
+                const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+                Vec<T, V> acc[3];
+                ku_row_fan<T, V, DIFF>(stage_rec(srec0, stage_bytes, sg),
+                                       stage_slab(sslab0, stage_bytes, sg), k0, k1, A.u, A.coef,
+                                       S, col, ua, acc);
+                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------ burst-gather step
@@ -1087,6 +1074,38 @@ int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, 
     }
 }
 
+template <typename K, typename T>
+int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStream_t st,
+                  const StepArgs<T>& A) {
+    if (smem > 48 * 1024) {
+        cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return fail(CVFES_ERR_CUDA, "k_step_fanp smem attribute: %s", cudaGetErrorString(e));
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+            cudaSuccess ||
+        per_sm <= 0)
+        return fail(CVFES_ERR_CUDA, "k_step_fanp: no resident block fits");
+    long long blocks = (long long)per_sm * sm_count();
+    if (blocks > n_items) blocks = n_items;
+    kernel<<<(unsigned)blocks, threads, smem, st>>>(A, n_items);
+    CVFES_LAUNCH_CHECK("k_step_fanp");
+    return CVFES_OK;
+}
+
+template <typename T, int V, bool DIFF>
+int launch_fanp(int minb, long long n_items, int threads, size_t smem, cudaStream_t st,
+                const StepArgs<T>& A) {
+    switch (minb) {
+        case 4: return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A);
+        case 3: return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A);
+        case 2: return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A);
+        default: return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A);
+    }
+}
+
 template <typename T, int V, bool DIFF, int MAXD>
 int launch_burst(int minb, dim3 g1, int threads, size_t smem, cudaStream_t st,
                  const StepArgs<T>& A) {
@@ -1101,6 +1120,11 @@ int launch_burst(int minb, dim3 g1, int threads, size_t smem, cudaStream_t st,
 template <typename T, int V, bool DIFF>
 int launch_staged_v(int variant, int minb, dim3 grid, int threads, size_t smem, cudaStream_t st,
                     const StepArgs<T>& A, long long max_degree = 0) {
+    if (variant == 6) {
+        const long long n_items = (long long)grid.x * grid.y;
+        const size_t smem2 = 16 + 2 * (smem - 16);
+        return launch_fanp<T, V, DIFF>(minb, n_items, threads, smem2, st, A);
+    }
     if (variant == 5 && max_degree > 0 && max_degree <= 8) {
         const dim3 g1((unsigned)((long long)grid.x * grid.y));
         if (max_degree <= 6) return launch_burst<T, V, DIFF, 6>(minb, g1, threads, smem, st, A);
@@ -1504,8 +1528,8 @@ extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: npb must be in 1..8");
     if (minb < 1 || minb > 4)
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: minb must be in 1..4");
-    if (staged < 0 || staged > 5)
-        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..5");
+    if (staged < 0 || staged > 6)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..6");
     StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
     t.vec = vec;
     t.npb = npb;

@@ -85,6 +85,19 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 }
 constexpr int kMaxPolls = 1 << 22;
 
+// Record and stiffness-row pointers of stage q of a two-stage shared-memory ring.
+template <typename P>
+__device__ __forceinline__ P* stage_ptr(P* base0, size_t stage_bytes, int q) {
+    return reinterpret_cast<P*>(reinterpret_cast<unsigned char*>(base0) + q * stage_bytes);
+}
+__device__ __forceinline__ int4* stage_rec(int4* base0, size_t stage_bytes, int q) {
+    return stage_ptr(base0, stage_bytes, q);
+}
+template <typename T>
+__device__ __forceinline__ T* stage_slab(T* base0, size_t stage_bytes, int q) {
+    return stage_ptr(base0, stage_bytes, q);
+}
+
 // Thread -> (node, sample vector).  A block holds `npb` consecutive nodes and
 // `tpn` consecutive sample vectors of each (tpn = min(S/VEC, 32)); blockIdx.y
 // picks the sample chunk, the last one partly filled when S/VEC is not a
@@ -223,6 +236,114 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
         }
         stcs<T, V>(A.un + row + d * S, o);
+    }
+}
+
+// ------------------------------------------------------------ fan-rotation row
+// The fan order makes the first neighbour of element k the second neighbour of
+// element k-1, so element k needs only one new neighbour row set.  Three register
+// buffers rotate through the roles (previous = first neighbour, current = second
+// neighbour, next = in flight); the slot loop is unrolled three times so the
+// rotation is a renaming, not a copy.  Neighbour rows are turned into differences
+// u_b - u_a once (FP32 form) and reused by the following element.
+template <typename T, int V>
+__device__ __forceinline__ void load_rows(Vec<T, V> (&x)[3], const T* __restrict__ u, int node,
+                                          size_t S, size_t col) {
+    const T* p = u + (size_t)node * 3 * S + col;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] = ldg<T, V>(p + d * S);
+}
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void to_diff(Vec<T, V> (&x)[3], const Vec<T, V> (&ua)[3]) {
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d] = vsub(x[d], ua[d]);
+    }
+}
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void slot_fma(const T* K, const Vec<T, V>& c, const Vec<T, V> (&d1)[3],
+                                         const Vec<T, V> (&d2)[3], const Vec<T, V> (&ua)[3],
+                                         Vec<T, V> (&acc)[3]) {
+    T kk[28];
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int q = (DIFF ? 2 : 0); q < 7; ++q) {
+            const float4 t = reinterpret_cast<const float4*>(K)[q];
+            kk[4 * q] = t.x;
+            kk[4 * q + 1] = t.y;
+            kk[4 * q + 2] = t.z;
+            kk[4 * q + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = (DIFF ? 4 : 0); q < 14; ++q) {
+            const double2 t = reinterpret_cast<const double2*>(K)[q];
+            kk[2 * q] = t.x;
+            kk[2 * q + 1] = t.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Vec<T, V> t = vzero<T, V>();
+        if constexpr (!DIFF) {
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) axpy(t, kk[3 * i + jj], ua[jj]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[9 + 3 * i + jj], d1[jj]);
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) axpy(t, kk[18 + 3 * i + jj], d2[jj]);
+        vfma(acc[i], c, t);
+    }
+}
+
+// One element of the fan: prev holds the first neighbour (difference), cur the
+// second one as loaded; the next element's row set is issued into nxt first.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void fan_phase(int& k, int k1, const int4* srec, const T* sslab,
+                                          const T* __restrict__ u, const T* __restrict__ coef,
+                                          size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                          Vec<T, V> (&acc)[3], Vec<T, V> (&prev)[3],
+                                          Vec<T, V> (&cur)[3], const Vec<T, V>& ccur,
+                                          Vec<T, V> (&nxt)[3], Vec<T, V>& cnxt) {
+    const bool more = k + 1 < k1;
+    int4 rn = make_int4(0, 0, 0, 1);
+    if (more) {
+        rn = srec[k + 1];
+        load_rows<T, V>(nxt, u, rn.z, S, col);
+        cnxt = ldg<T, V>(coef + (size_t)rn.x * S + col);
+    }
+    to_diff<T, V, DIFF>(cur, ua);
+    slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, prev, cur, ua, acc);
+    if (more && !(rn.w & 1)) {  // fan break: the next element's first neighbour is new
+        load_rows<T, V>(cur, u, rn.y, S, col);
+        to_diff<T, V, DIFF>(cur, ua);
+    }
+    ++k;
+}
+
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row_fan(const int4* srec, const T* sslab, int k0, int k1,
+                                           const T* __restrict__ u, const T* __restrict__ coef,
+                                           size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                           Vec<T, V> (&acc)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    if (k0 >= k1) return;
+    Vec<T, V> B0[3], B1[3], B2[3], c0, c1, c2;
+    const int4 r0 = srec[k0];
+    load_rows<T, V>(B0, u, r0.y, S, col);
+    load_rows<T, V>(B1, u, r0.z, S, col);
+    c1 = ldg<T, V>(coef + (size_t)r0.x * S + col);
+    to_diff<T, V, DIFF>(B0, ua);
+    int k = k0;
+    while (true) {
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B0, B1, c1, B2, c2);
+        if (k >= k1) break;
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B1, B2, c2, B0, c0);
+        if (k >= k1) break;
+        fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B2, B0, c0, B1, c1);
+        if (k >= k1) break;
     }
 }
 

@@ -108,42 +108,43 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
 
 def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
                grids: Optional[Sequence[int]] = None, steps: int = 48,
-               use_cache: bool = True) -> dict:
-    """Pick the batch's samples per thread and persistent grid size."""
+               use_cache: bool = True, variants: Optional[Sequence[int]] = None) -> dict:
+    """Pick the batch's kernel, samples per thread and persistent grid size."""
     dev = batch.device
     shape = ("batch", batch.precision, tuple((s.lclNNodes, s.nElms, s.nSmp) for s in batch.solvers))
     key = _key("batch", dev, shape)
     cache = _load_cache() if use_cache else {}
     if key in cache:
         best = cache[key]
-        batch.set_launch(vec=best["vec"], grid=best["grid"])
+        batch.set_launch(vec=best["vec"], grid=best["grid"], variant=best.get("variant", 0))
         return dict(best, cached=True)
+    if variants is None:
+        variants = [1, 0] if batch.totals[2] > 0 else [0]
     maxv = 4 if batch.precision == 32 else 2
     if vecs is None:
         vecs = [v for v in (4, 2, 1) if v <= maxv and all(s.nSmp % v == 0 for s in batch.solvers)]
-    if grids is None:
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        grids = [0, 4 * sms, 8 * sms, 16 * sms]
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    grid_sets = {0: list(grids) if grids is not None else [0, 4 * sms, 8 * sms, 16 * sms],
+                 1: list(grids) if grids is not None else [0, 4 * sms]}
     saved = [[b.clone() for b in s.bufs] for s in batch.solvers]
     rot0 = batch.rot
     pres = np.zeros(steps + batch.graph_chunk + 2)
     results = []
-    for vec in vecs:
-        for grid in grids:
-            batch.set_launch(vec=vec, grid=grid)
-            for s, sv in zip(batch.solvers, saved):
-                for b, x in zip(s.bufs, sv):
-                    b.copy_(x)
-            batch.rot = rot0
-            batch.Advance(pres[:batch.graph_chunk + 2])
-            ms = _time_ms(lambda: batch.Advance(pres[:steps]), dev) / steps
-            results.append((ms, dict(vec=vec, grid=grid, ms_per_step=ms)))
+    for variant, vec, grid in [(v, x, g) for v in variants for x in vecs for g in grid_sets[v]]:
+        batch.set_launch(vec=vec, grid=grid, variant=variant)
+        for s, sv in zip(batch.solvers, saved):
+            for b, x in zip(s.bufs, sv):
+                b.copy_(x)
+        batch.rot = rot0
+        batch.Advance(pres[:batch.graph_chunk + 2])
+        ms = _time_ms(lambda: batch.Advance(pres[:steps]), dev) / steps
+        results.append((ms, dict(variant=variant, vec=vec, grid=grid, ms_per_step=ms)))
     for s, sv in zip(batch.solvers, saved):
         for b, x in zip(s.bufs, sv):
             b.copy_(x)
     batch.rot = rot0
     best = min(results, key=lambda r: r[0])[1]
-    batch.set_launch(vec=best["vec"], grid=best["grid"])
+    batch.set_launch(vec=best["vec"], grid=best["grid"], variant=best["variant"])
     cur = (3 - batch.rot) % 3
     for s in batch.solvers:
         s.cur, s.prev, s.nxt = cur, (cur + 1) % 3, (cur + 2) % 3

@@ -272,10 +272,15 @@ int cvfes_graph_destroy(cvfes_graph* g);
  * batched form of the per-step solid path; the reference runs one mesh per MPI
  * rank, physicsSolverSDampGPUs.py:325-399).  The caller allocates a device table of
  * cvfes_batch_table_bytes(n) bytes; cvfes_batch_pack fills it (synchronous copy)
- * and returns the number of work items.  All meshes rotate their buffers in lock
- * step: with rot = (steps taken) % 3, u_n = buf[(3-rot)%3], u_{n-1} = buf[(4-rot)%3].
- * vec: samples per thread (FP32 1|2|4, FP64 1|2), must divide every mesh's S.
- * grid: blocks of the persistent launch (<= 0: one block per work item).       */
+ * and writes totals[3]: [0] work items of the gather kernel (variant 0), [1] work
+ * items of the fan kernel (variant 1: blocks of 2 warps, slot rows staged by TMA
+ * into two shared-memory stages, fan-rotation gathers), [2] the fan kernel's stage
+ * capacity in slots (-1 when a mesh has no max_degree).  All meshes rotate their
+ * buffers in lock step: with rot = (steps taken) % 3, u_n = buf[(3-rot)%3],
+ * u_{n-1} = buf[(4-rot)%3].  vec: samples per thread (FP32 1|2|4, FP64 1|2), must
+ * divide every mesh's S.  grid: blocks of the persistent launch (<= 0: one block per
+ * work item for variant 0, as many as fit for variant 1).  Both variants give the
+ * same bits as the single-mesh kernels.                                          */
 typedef struct cvfes_batch_item {
     cvfes_solid_mesh mesh;       /* descriptor of this mesh (device arrays)     */
     const void*      coef;       /* [E][S] T                                    */
@@ -288,17 +293,18 @@ typedef struct cvfes_batch_item {
 
 int64_t cvfes_batch_table_bytes(int32_t n_meshes);
 int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes, int32_t precision,
-                     int32_t vec, void* table_dev, int64_t* total_items);
-int cvfes_batch_step(const void* table_dev, int32_t n_meshes, int64_t total_items,
-                     int32_t precision, int32_t vec, int32_t rot, const int64_t* clock,
-                     int64_t j, int32_t grid, void* stream);
-int cvfes_batch_advance(const void* table_dev, int32_t n_meshes, int64_t total_items,
-                        int32_t precision, int32_t vec, int32_t rot0, int64_t* clock,
-                        int64_t n_steps, int32_t grid, int32_t* rot_out, void* stream);
+                     int32_t vec, void* table_dev, int64_t* totals);
+int cvfes_batch_step(const void* table_dev, int32_t n_meshes, const int64_t* totals,
+                     int32_t precision, int32_t vec, int32_t variant, int32_t rot,
+                     const int64_t* clock, int64_t j, int32_t grid, void* stream);
+int cvfes_batch_advance(const void* table_dev, int32_t n_meshes, const int64_t* totals,
+                        int32_t precision, int32_t vec, int32_t variant, int32_t rot0,
+                        int64_t* clock, int64_t n_steps, int32_t grid, int32_t* rot_out,
+                        void* stream);
 /* `chunk` batched steps (multiple of 3) and the clock increment as one graph. */
-int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, int64_t total_items,
-                              int32_t precision, int32_t vec, int64_t* clock, int64_t chunk,
-                              int32_t grid, cvfes_graph** out);
+int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, const int64_t* totals,
+                              int32_t precision, int32_t vec, int32_t variant, int64_t* clock,
+                              int64_t chunk, int32_t grid, cvfes_graph** out);
 
 /* ------------------------------------------------------------ geometric update
  * Stiffness and follower pressure on the deformed geometry x + u_g of each sample:

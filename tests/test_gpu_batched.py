@@ -33,10 +33,15 @@ class _Cfg:
 
 
 @pytest.mark.parametrize("precision", [32, 64])
-def test_batch_equals_meshes_advanced_alone(lib, cuda, precision):
+@pytest.mark.parametrize("variant", [0, 1])
+def test_batch_equals_meshes_advanced_alone(lib, cuda, precision, variant):
+    """Row-gather (0) and fan (1) batch kernels, meshes of 16..128 samples (several nodes
+    per warp in the fan layout): the bits of each mesh advanced alone."""
     cases, meshes, dts = small_batch()
     pres = 1.33e5 * np.minimum(np.arange(100) / 100.0, 1.0)
-    batch = BatchedSolidSolver(meshes, dts, precision=precision, device=cuda, graph_chunk=24)
+    batch = BatchedSolidSolver(meshes, dts, precision=precision, device=cuda, graph_chunk=24,
+                               variant=variant)
+    assert batch.variant == variant
     batch.Advance(pres[:37], use_graph=True)     # graph chunks + plain remainder
     batch.Advance(pres[37:100], use_graph=True)  # starts at a non-zero rotation
     saved = _lib.get_step_tuning(precision)
