@@ -45,6 +45,15 @@ class SolidMeshDesc(C.Structure):
         ("fhat", C.c_void_p),
         ("max_degree", C.c_int64),
         ("status", C.c_void_p),
+        ("tile_win", C.c_void_p),
+        ("tile_rec", C.c_void_p),
+        ("node_loc", C.c_void_p),
+        ("tile_p", C.c_int32),
+        ("tile_h", C.c_int32),
+        ("tile_w", C.c_int32),
+        ("tile_eh", C.c_int32),
+        ("tile_we", C.c_int32),
+        ("tile_pad", C.c_int32),
     ]
 
 
@@ -132,6 +141,7 @@ SIGNATURES = {
                                       C.POINTER(C.c_int32), P]),
     "cvfes_batch_graph_capture": (C.c_int, [P, I32, P, I32, I32, I32, P, I64, I32,
                                             C.POINTER(C.c_void_p)]),
+    "cvfes_mesh_tiles": (C.c_int, [I64, I64, P, P, I64, I32, I32, I32, I32, I32, P, P, P, P]),
     "cvfes_solid_slot_geometry_f64": (C.c_int, [I64, P, P, P, P, P, P]),
     "cvfes_solid_step_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),
     "cvfes_solid_step_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),

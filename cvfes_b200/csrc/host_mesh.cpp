@@ -142,3 +142,88 @@ extern "C" int cvfes_mesh_color_greedy(int64_t n_nodes, int64_t n_elems, const i
     }
     return used_colors;
 }
+
+namespace {
+
+// Cover the sorted distinct ids with at most `max_w` windows of `h` consecutive ids,
+// greedily from the smallest uncovered id (the fewest windows for fixed-length
+// intervals); returns the window starts.
+std::vector<int32_t> cover_windows(const std::vector<int32_t>& ids, int32_t h, int32_t max_w) {
+    std::vector<int32_t> starts;
+    size_t i = 0;
+    while (i < ids.size() && (int32_t)starts.size() < max_w) {
+        const int32_t s = ids[i];
+        starts.push_back(s);
+        while (i < ids.size() && ids[i] < s + h) ++i;
+    }
+    return starts;
+}
+
+// Shared-memory row of id within the windows (window k holds ids [starts[k], +h)),
+// or -1 - id when no window holds it.
+int32_t window_loc(const std::vector<int32_t>& starts, int32_t h, int32_t id) {
+    for (size_t k = 0; k < starts.size(); ++k)
+        if (id >= starts[k] && id < starts[k] + h) return (int32_t)k * h + (id - starts[k]);
+    return -1 - id;
+}
+
+}  // namespace
+
+extern "C" int cvfes_mesh_tiles(int64_t n_nodes, int64_t n_elems, const int32_t* node_ptr,
+                                const int32_t* slot_rec, int64_t n_clamped, int32_t P, int32_t H,
+                                int32_t W, int32_t EH, int32_t WE, int32_t* tile_win,
+                                int32_t* tile_rec, int32_t* node_loc, int64_t* stats) {
+    if (n_nodes <= 0 || n_elems <= 0 || !node_ptr || !slot_rec || !tile_win || !tile_rec ||
+        !node_loc || !stats || P < 1 || H < P || W < 1 || EH < 1 || WE < 1 || n_clamped < 0 ||
+        n_clamped > n_nodes)
+        return cvfes::fail(CVFES_ERR_ARG, "cvfes_mesh_tiles: bad argument");
+    const int64_t n_tiles = (n_nodes + P - 1) / P;
+    const int nw = W + WE;
+    int64_t out_nodes = 0, out_elems = 0, max_need = 0;
+    std::vector<int32_t> nid, eid;
+    for (int64_t t = 0; t < n_tiles; ++t) {
+        const int64_t a0 = t * P, a1 = std::min<int64_t>(a0 + P, n_nodes);
+        nid.clear();
+        eid.clear();
+        for (int64_t a = std::max<int64_t>(a0, n_clamped); a < a1; ++a) {
+            nid.push_back((int32_t)a);
+            for (int32_t k = node_ptr[a]; k < node_ptr[a + 1]; ++k) {
+                eid.push_back(slot_rec[4 * (int64_t)k]);
+                nid.push_back(slot_rec[4 * (int64_t)k + 1]);
+                nid.push_back(slot_rec[4 * (int64_t)k + 2]);
+            }
+        }
+        std::sort(nid.begin(), nid.end());
+        nid.erase(std::unique(nid.begin(), nid.end()), nid.end());
+        std::sort(eid.begin(), eid.end());
+        eid.erase(std::unique(eid.begin(), eid.end()), eid.end());
+        const std::vector<int32_t> ns = cover_windows(nid, H, W);
+        const std::vector<int32_t> es = cover_windows(eid, EH, WE);
+        const int64_t need = (int64_t)cover_windows(nid, H, 1 << 20).size();
+        max_need = std::max(max_need, need);
+        for (int k = 0; k < nw; ++k) tile_win[t * nw + k] = -1;
+        for (size_t k = 0; k < ns.size(); ++k) tile_win[t * nw + k] = ns[k];
+        for (size_t k = 0; k < es.size(); ++k) tile_win[t * nw + W + k] = es[k];
+        for (int64_t a = a0; a < a1; ++a) {
+            const bool live = a >= n_clamped;
+            node_loc[a] = live ? window_loc(ns, H, (int32_t)a) : -1 - (int32_t)a;
+            for (int32_t k = node_ptr[a]; k < node_ptr[a + 1]; ++k) {
+                const int64_t q = 4 * (int64_t)k;
+                const int32_t e = slot_rec[q], b1 = slot_rec[q + 1], b2 = slot_rec[q + 2];
+                tile_rec[q] = live ? window_loc(es, EH, e) : -1 - e;
+                tile_rec[q + 1] = live ? window_loc(ns, H, b1) : -1 - b1;
+                tile_rec[q + 2] = live ? window_loc(ns, H, b2) : -1 - b2;
+                tile_rec[q + 3] = slot_rec[q + 3];
+                if (live) {
+                    out_elems += tile_rec[q] < 0;
+                    out_nodes += (tile_rec[q + 1] < 0) + (tile_rec[q + 2] < 0);
+                }
+            }
+        }
+    }
+    stats[0] = n_tiles;
+    stats[1] = out_nodes;
+    stats[2] = out_elems;
+    stats[3] = max_need;
+    return CVFES_OK;
+}

@@ -1189,10 +1189,16 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     A.status = m->status;
     A.cap_slots = 0;
     const void* ptrs[6] = {coef, invm, u, up, un, nullptr};
-    const StepTuning& tune = tuning_of<T>();
+    StepTuning tune = tuning_of<T>();
     int V = pick_vec<T>(ptrs, 5, A.S);
     while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
+    if (tune.staged == 7) {  // TMA-tiled strips; the fan kernel where they do not apply
+        const int trc = launch_step_tile<T>(m, A, tune.vec, st);
+        if (trc <= 0) return trc;
+        tune.staged = 3;
+        tune.minb = 2;
+    }
     // Pipelined persistent kernel (npb = warps per block, minb = stages per warp).
     if (tune.staged == 4 && m->max_degree > 0 && m->max_degree <= 32 && (A.S / V) % 32 == 0) {
         A.nch = A.S / V / 32;
@@ -1528,8 +1534,8 @@ extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: npb must be in 1..8");
     if (minb < 1 || minb > 4)
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: minb must be in 1..4");
-    if (staged < 0 || staged > 6)
-        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..6");
+    if (staged < 0 || staged > 7)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..7");
     StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
     t.vec = vec;
     t.npb = npb;

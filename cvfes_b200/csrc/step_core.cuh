@@ -217,7 +217,30 @@ __device__ __forceinline__ void node_load(const StepArgs<T>& A, long long a, T p
     (void)q;
 }
 
-// Fused update of one node row (increment form, see the file header) and its store.
+// Fused update of one node row (increment form, see the file header) and its store,
+// from the row's u_{n-1} and inverse mass already in registers.
+template <typename T, int V>
+__device__ __forceinline__ void step_update(const StepArgs<T>& A, size_t S, size_t row,
+                                            const Vec<T, V> (&ua)[3], const Vec<T, V> (&acc)[3],
+                                            const T (&f)[3], const Vec<T, V> (&ups)[3],
+                                            const Vec<T, V>& im) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const Vec<T, V>& up = ups[d];
+        const T load = f[d];
+        Vec<T, V> o;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const T dv = ua[d].v[i] - up.v[i];
+            const T w = A.w0 * im.v[i];
+            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+        }
+        stcs<T, V>(A.un + row + d * S, o);
+    }
+}
+
+// As step_update, reading the row's u_{n-1} and inverse mass here.
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
@@ -346,6 +369,12 @@ __device__ __forceinline__ void ku_row_fan(const int4* srec, const T* sslab, int
         if (k >= k1) break;
     }
 }
+
+// TMA-tiled step (solid_tile.cu): returns 1 without launching when the mesh has no
+// tiling or the shape does not fit the tiled kernel.
+template <typename T>
+int launch_step_tile(const cvfes_solid_mesh* m, const StepArgs<T>& A, int vec_max,
+                     cudaStream_t st);
 
 }  // namespace cvfes
 

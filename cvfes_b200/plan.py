@@ -120,6 +120,25 @@ class SolidPlan:
                  ptr(self.slot_k32), ptr(self.kt_full), ptr(self.area), ptr(self.normal),
                  self._s())
         self.S = None
+        self.build_tiles()
+
+    def build_tiles(self, P: int = 16, H: int = 18, W: int = 3, EH: int = 36, WE: int = 2):
+        """Strip tiling for the TMA-tiled step (``cvfes_mesh_tiles``): tiles of P nodes,
+        W windows of H node ids and WE windows of EH element ids per tile."""
+        nt = (self.N + P - 1) // P
+        tw = np.empty((nt, W + WE), dtype=np.int32)
+        tr = np.empty((3 * self.E, 4), dtype=np.int32)
+        nl = np.empty(self.N, dtype=np.int32)
+        st = np.zeros(4, dtype=np.int64)
+        call("cvfes_mesh_tiles", self.N, self.E, ptr(self.host_node_ptr), ptr(self.host_slot_rec),
+             self.n_clamped, P, H, W, EH, WE, ptr(tw), ptr(tr), ptr(nl), ptr(st))
+        dev = self.device
+        self.tile_win = torch.from_numpy(tw).to(dev)
+        self.tile_rec = torch.from_numpy(tr).to(dev)
+        self.node_loc = torch.from_numpy(nl).to(dev)
+        self.tile_shape = (P, H, W, EH, WE)
+        self.tile_stats = dict(tiles=int(st[0]), node_outliers=int(st[1]),
+                               element_outliers=int(st[2]), most_windows=int(st[3]))
 
     def _s(self):
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -171,9 +190,15 @@ class SolidPlan:
         fhat = self.fhat64 if precision == 64 else self.fhat32
         if slab is None:
             raise RuntimeError(f"plan was built without FP{precision} templates")
-        return _lib.SolidMeshDesc(self.N, self.E, self.S, self.n_clamped, self.clamp_value,
-                                  ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat),
-                                  self.max_degree, ptr(self.status))
+        d = _lib.SolidMeshDesc(self.N, self.E, self.S, self.n_clamped, self.clamp_value,
+                               ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat),
+                               self.max_degree, ptr(self.status))
+        if getattr(self, "tile_win", None) is not None:
+            P, H, W, EH, WE = self.tile_shape
+            d.tile_win, d.tile_rec, d.node_loc = (ptr(self.tile_win), ptr(self.tile_rec),
+                                                  ptr(self.node_loc))
+            d.tile_p, d.tile_h, d.tile_w, d.tile_eh, d.tile_we = P, H, W, EH, WE
+        return d
 
     def check_status(self):
         """Raise if a bounded device wait gave up since the last check (syncs the stream)."""

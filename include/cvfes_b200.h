@@ -58,6 +58,17 @@ typedef struct cvfes_solid_mesh {
     int64_t        max_degree;    /* max slots of one node (0: unknown -> no smem staging) */
     int32_t*       status;        /* device int32 or NULL: bit 0 set when a bounded
                                      device wait gave up (read by cvfes_status_read) */
+    /* Strip tiling of the TMA-tiled step (staged = 7), from cvfes_mesh_tiles, device
+     * arrays; tile_win NULL: no tiling (the tiled variant falls back to the fan).   */
+    const int32_t* tile_win;      /* [n_tiles][tile_w + tile_we] window starts      */
+    const int32_t* tile_rec;      /* [4 * n_slots] shared-memory rows of each slot  */
+    const int32_t* node_loc;      /* [n_nodes] shared-memory row of each node       */
+    int32_t        tile_p;        /* nodes per tile                                 */
+    int32_t        tile_h;        /* node ids per node window                       */
+    int32_t        tile_w;        /* node windows per tile (at most 4)              */
+    int32_t        tile_eh;       /* element ids per element window                 */
+    int32_t        tile_we;       /* element windows per tile (at most 3)           */
+    int32_t        tile_pad;
 } cvfes_solid_mesh;
 
 /* Step-kernel tuning (the autotuner sets these; defaults: variant 3, FP32 vec 4,
@@ -77,6 +88,15 @@ typedef struct cvfes_solid_mesh {
  *           5 = as 1, with the node's whole gather (every neighbour row and
  *               coefficient row) requested before the first product (meshes of
  *               node degree <= 8; otherwise as 3);
+ *           6 = as 3, persistent, the next work item's slot rows staged while the
+ *               current one is multiplied (two shared-memory stages);
+ *           7 = TMA-tiled: a block owns a strip of tile_p nodes and one sample chunk
+ *               (64 FP32 / 32 FP64 samples); 2D TMA tensor copies stage the strip's
+ *               node windows (all neighbour rows) and element windows (coefficient
+ *               rows), with its slot rows, into a ring of shared-memory stages; the
+ *               products read shared memory (ids outside the windows read global
+ *               memory).  Needs the mesh's tiling (cvfes_mesh_tiles) and S a multiple
+ *               of the chunk; otherwise as 3.  vec caps the chunk (vec 1: 32 samples);
  *   minb: resident blocks per SM the register allocation must allow (1..4).
  * Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,
@@ -100,6 +120,24 @@ int         cvfes_version(void);
  * node_ptr [N+1]; slot_rec [4*3E]; elem_slot [3E] (slot of (e, local node)). */
 int cvfes_mesh_incidence(int64_t n_nodes, int64_t n_elems, const int64_t* elems,
                          int32_t* node_ptr, int32_t* slot_rec, int32_t* elem_slot);
+
+/* Strip tiling for the TMA-tiled step: tile t holds nodes [t*P, (t+1)*P).  For the
+ * unclamped nodes of each tile, windows of H consecutive node ids covering the nodes
+ * and all their neighbours (at most W, greedily from the smallest uncovered id) and
+ * windows of EH element ids covering their elements (at most WE).  Outputs (host):
+ *   tile_win int32 [n_tiles][W+WE]: node window starts, then element window starts
+ *            (-1: unused);
+ *   tile_rec int32 [4*3E]: per slot, the shared-memory row of its element, first
+ *            and second neighbour within the tile's windows (window k, offset i ->
+ *            k*H + i, elements k*EH + i), or -1 - id when no window holds it; then the
+ *            slot's flags;
+ *   node_loc int32 [N]: the row of the node itself, or -1 - id;
+ *   stats int64 [4]: tiles, neighbour references outside the windows, element
+ *            references outside the windows, most windows a tile would need.     */
+int cvfes_mesh_tiles(int64_t n_nodes, int64_t n_elems, const int32_t* node_ptr,
+                     const int32_t* slot_rec, int64_t n_clamped, int32_t P, int32_t H, int32_t W,
+                     int32_t EH, int32_t WE, int32_t* tile_win, int32_t* tile_rec,
+                     int32_t* node_loc, int64_t* stats);
 
 /* Greedy element colouring over the node-sharing graph, smallest free colour
  * in element order (meshColoring.py:7-63).  colors: host int32 [E].

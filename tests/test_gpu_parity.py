@@ -207,15 +207,18 @@ def test_invalid_arguments_are_rejected(lib, cuda):
 
 
 VARIANTS = {32: [(0, 4, 8, 1), (1, 4, 4, 2), (2, 4, 4, 2), (3, 4, 2, 2), (4, 4, 4, 2), (4, 4, 4, 3),
-                 (4, 2, 8, 3), (3, 2, 4, 3), (1, 1, 8, 4)],
-            64: [(0, 2, 8, 1), (1, 2, 4, 2), (3, 2, 2, 2), (4, 2, 4, 2), (4, 1, 6, 3), (3, 1, 4, 3)]}
+                 (4, 2, 8, 3), (3, 2, 4, 3), (1, 1, 8, 4), (6, 4, 2, 1), (7, 2, 2, 2),
+                 (7, 1, 2, 2)],
+            64: [(0, 2, 8, 1), (1, 2, 4, 2), (3, 2, 2, 2), (4, 2, 4, 2), (4, 1, 6, 3), (3, 1, 4, 3),
+                 (6, 2, 4, 2), (7, 1, 2, 2)]}
 
 
 @pytest.mark.parametrize("precision", [32, 64])
 def test_step_kernel_variants_are_bitwise_identical(lib, cuda, precision):
     """Every step-kernel variant (L1 gather, TMA-staged, cp.async gather, fan rotation,
-    pipelined persistent) computes the same floating-point operations in the same
-    order: their states after 60 steps must be bitwise equal."""
+    pipelined persistent, persistent fan, TMA-tiled strips) computes the same
+    floating-point operations in the same order: their states after 60 steps must be
+    bitwise equal."""
     from cvfes_b200.cases import CASES
     case = CASES["tube64x128"]
     S = 128 if precision == 32 else 64
@@ -421,3 +424,29 @@ def test_traction_series_input_against_oracle(lib, cuda, tmp_path, constant):
         p = 5e4 if t > T else 5e4 * t / T  # the configuration's linear ramp
         o.step(p, tr)
     assert so.rel_l2(solver.displacement(), o.u) < FP64_TOL
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_tiled_step_with_outliers_matches_fan(lib, cuda, precision):
+    """The TMA-tiled step with one node window and one element window per tile, so most
+    neighbour and coefficient rows are read from global memory: the fan kernel's bits."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    S = 128 if precision == 32 else 64
+    mesh = c0_mesh(S)
+    pres = case.pressures(36)
+    saved = _lib.get_step_tuning(precision)
+    try:
+        _lib.set_step_tuning(precision, 4 if precision == 32 else 2, 2, 3, 2)
+        ref = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+        ref.Advance(pres)
+        _lib.set_step_tuning(precision, 2 if precision == 32 else 1, 2, 7, 2)
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+        s.plan.build_tiles(P=16, H=18, W=1, EH=36, WE=1)
+        assert s.plan.tile_stats["node_outliers"] > 0 and s.plan.tile_stats["element_outliers"] > 0
+        s._desc = s.plan.desc(precision)
+        s.Advance(pres)
+        s.plan.check_status()
+    finally:
+        _lib.set_step_tuning(precision, **saved)
+    assert torch.equal(s.local_displacement(), ref.local_displacement())
