@@ -80,7 +80,7 @@ class MismatchProblem:
             self._mesh_desc = plan.desc(precision)
             dt_ = self.dtype
             z = lambda *shape, dtype=dt_: torch.zeros(shape, dtype=dtype, device=dev)
-            self.own = z(E * 28)
+            self.own = z(3 * E * 28)  # per slot; the owner slot of each element holds its blocks
             call("cvfes_adjoint_owner_blocks", self._mesh_desc, precision, ptr(plan.elems),
                  ptr(plan.elem_slot), ptr(self.own), self._stream())
             self.logE = z(E, S, dtype=torch.float64)

@@ -42,7 +42,9 @@ struct MassWeights {
     double w[9];  // w[3a + g]: lumped-mass weight of local node a at quadrature point g
 };
 
-// Owner-slot neighbour blocks of every element, in the owner slot's (b1, b2) order.
+// Owner-slot neighbour blocks of every element, in the owner slot's (b1, b2) order,
+// stored at the owner slot (the slot of the element's local node 0); the entries of the
+// other slots are not used.
 template <typename T>
 __global__ void k_owner_blocks(long long n_elems, const int32_t* __restrict__ elems,
                                const int32_t* __restrict__ elem_slot,
@@ -55,7 +57,7 @@ __global__ void k_owner_blocks(long long n_elems, const int32_t* __restrict__ el
     const int l1 = elems[3 * e + 1] == b1 ? 1 : 2;
     const int s1 = elem_slot[3 * e + l1], s2 = elem_slot[3 * e + 3 - l1];
     const int q = slot_rec[4 * s1 + 1] == b2 ? 1 : 2;  // block of b2 in b1's slot
-    T* o = own + (size_t)kOwnStride * e;
+    T* o = own + (size_t)kOwnStride * s0;
     const T* k1 = slab + (size_t)kSlabStride * s1;
     const T* k2 = slab + (size_t)kSlabStride * s2;
 #pragma unroll
@@ -193,7 +195,8 @@ __device__ __forceinline__ void load27(const T* K, T (&kk)[27]) {
 // the first and second neighbour rows of u_n and chi_{n+1}, already differences
 // u_b - u_a in the DIFF form, raw rows otherwise.
 template <typename T, int V, bool DIFF>
-__device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, size_t S, size_t col,
+__device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, const T* own, size_t S,
+                                           size_t col,
                                            const Vec<T, V> (&u1)[3], const Vec<T, V> (&u2)[3],
                                            const Vec<T, V> (&x1)[3], const Vec<T, V> (&x2)[3],
                                            const Vec<T, V> (&ua)[3], const Vec<T, V> (&ca)[3]) {
@@ -212,8 +215,11 @@ __device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, size_t S,
             dy2[d] = vsub(x2[d], ca[d]);
         }
     }
+    // own points into global memory (gather kernel) or shared memory (fan kernel): plain
+    // generic loads, not the global-only read-only path
     T ob[27];
-    load27<T>(A.own + (size_t)kOwnStride * e, ob);
+#pragma unroll
+    for (int i = 0; i < 27; ++i) ob[i] = own[i];
     Vec<T, V> g = vzero<T, V>();
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -366,7 +372,9 @@ __global__ void __launch_bounds__(256) k_reverse(RevArgs<T> A) {
             vfma(accU[i], c, tu);
             vfma(accC[i], c, tc);
         }
-        if (((r.w >> 8) & 3) == 0) owner_grad<T, V, DIFF>(A, r.x, S, col, x1, x2, y1, y2, ua, ca);
+        if (((r.w >> 8) & 3) == 0)
+            owner_grad<T, V, DIFF>(A, r.x, A.own + (size_t)kOwnStride * k, S, col, x1, x2, y1, y2,
+                                   ua, ca);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             cu[d] = x2[d];
@@ -448,7 +456,7 @@ __device__ __forceinline__ void slot_fma2(const T* K, const Vec<T, V>& c,
 
 template <typename T, int V, bool DIFF>
 __device__ __forceinline__ void rev_phase(int& k, int k1, const int4* srec, const T* sslab,
-                                          const RevArgs<T>& A, size_t S, size_t col,
+                                          const T* sown, const RevArgs<T>& A, size_t S, size_t col,
                                           const Vec<T, V> (&ua)[3], const Vec<T, V> (&ca)[3],
                                           Vec<T, V> (&accU)[3], Vec<T, V> (&accC)[3],
                                           Vec<T, V> (&pu)[3], Vec<T, V> (&px)[3],
@@ -468,7 +476,9 @@ __device__ __forceinline__ void rev_phase(int& k, int k1, const int4* srec, cons
     const int4 r = srec[k];
     slot_fma2<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, pu, cu, px, cx, ua, ca, accU,
                           accC);
-    if (((r.w >> 8) & 3) == 0) owner_grad<T, V, DIFF>(A, r.x, S, col, pu, cu, px, cx, ua, ca);
+    if (((r.w >> 8) & 3) == 0)
+        owner_grad<T, V, DIFF>(A, r.x, sown + (size_t)kOwnStride * k, S, col, pu, cu, px, cx, ua,
+                               ca);
     if (more && !(rn.w & 1)) {  // fan break: the next slot's first neighbour is new
         load3<T, V>(cu, A.u, rn.y, S, col);
         load3<T, V>(cx, A.x, rn.y, S, col);
@@ -496,15 +506,17 @@ __global__ void __launch_bounds__(256, MINB) k_reverse_fan(RevArgs<T> A) {
     const uint32_t bar = smem_u32(smem);
     int4* srec = reinterpret_cast<int4*>(smem + 16);
     T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    T* sown = sslab + (size_t)A.cap_slots * kSlabStride;
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t b_rec = (uint32_t)nsl * 16u;
         const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
-        mbar_arrive_expect_tx(bar, b_rec + b_slab);
+        mbar_arrive_expect_tx(bar, b_rec + 2 * b_slab);
         if (nsl > 0) {
             bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
             bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+            bulk_g2s(smem_u32(sown), A.own + (size_t)kb * kOwnStride, b_slab, bar);
         }
     }
     const long long a = a0 + warp;
@@ -547,13 +559,13 @@ __global__ void __launch_bounds__(256, MINB) k_reverse_fan(RevArgs<T> A) {
         diff3<T, V, DIFF>(X0, ca);
         int k = k0;
         while (true) {
-            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U0, X0, U1,
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC, U0, X0, U1,
                                   X1, c1, U2, X2, c2);
             if (k >= k1) break;
-            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U1, X1, U2,
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC, U1, X1, U2,
                                   X2, c2, U0, X0, c0);
             if (k >= k1) break;
-            rev_phase<T, V, DIFF>(k, k1, srec, sslab, A, S, col, ua, ca, accU, accC, U2, X2, U0,
+            rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC, U2, X2, U0,
                                   X0, c0, U1, X1, c1);
             if (k >= k1) break;
         }
@@ -692,7 +704,7 @@ int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T*
     A.nch = 1;
     A.cap_slots = 0;
     const long long cap = (long long)tu.npb * m->max_degree;
-    const size_t smem = 16 + (size_t)cap * (16 + kSlabStride * sizeof(T));
+    const size_t smem = 16 + (size_t)cap * (16 + (kSlabStride + kOwnStride) * sizeof(T));
     const bool fan = tu.variant == 1 && m->max_degree > 0 && (A.S / V) % 32 == 0 &&
                      smem <= kRevMaxStage && tu.npb >= 1 && tu.npb <= 8;
     unsigned fan_grid = 0;

@@ -422,7 +422,7 @@ typedef struct cvfes_adjoint_desc {
                                      into obs instead of adding up J                 */
     const void*  coef;            /* [E][S] E*h                                      */
     const void*  invm;            /* [N][S] inverse lumped mass                      */
-    const void*  owner_blocks;    /* [E][28] from cvfes_adjoint_owner_blocks         */
+    const void*  owner_blocks;    /* [3E][28] from cvfes_adjoint_owner_blocks        */
     void*        state[3];        /* [3N][S] forward ring; final roles are returned  */
     void*        adj[2];          /* [3N][S] adjoint pair                            */
     void*        ckpt;            /* [ckpt_count][2][3N][S]                          */
@@ -455,7 +455,8 @@ int64_t cvfes_adjoint_ckpt_count(int64_t n_steps, int64_t ckpt_every);
 int64_t cvfes_adjoint_jpart_size(int64_t n_steps, int32_t obs_every, int32_t n_obs,
                                  int64_t n_samples);
 /* Per element, the blocks K_b1b1, K_b1b2, K_b2b2 of the unit stiffness in the order of
- * the slot of its local node 0 (elems [E][3] int32, elem_slot [E][3] int32). */
+ * the slot of its local node 0, stored at that slot: out [3E][28] (the other slots'
+ * entries are not written; elems [E][3] int32, elem_slot [E][3] int32). */
 int cvfes_adjoint_owner_blocks(const cvfes_solid_mesh* mesh, int32_t precision,
                                const int32_t* elems, const int32_t* elem_slot, void* out,
                                void* stream);
