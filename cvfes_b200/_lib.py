@@ -142,6 +142,8 @@ SIGNATURES = {
     "cvfes_batch_graph_capture": (C.c_int, [P, I32, P, I32, I32, I32, P, I64, I32,
                                             C.POINTER(C.c_void_p)]),
     "cvfes_mesh_tiles": (C.c_int, [I64, I64, P, P, I64, I32, I32, I32, I32, I32, P, P, P, P]),
+    "cvfes_set_geo_tuning": (C.c_int, [I32, I32, I32]),
+    "cvfes_get_geo_tuning": (C.c_int, [I32, P, P]),
     "cvfes_solid_slot_geometry_f64": (C.c_int, [I64, P, P, P, P, P, P]),
     "cvfes_solid_step_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),
     "cvfes_solid_step_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),

@@ -155,6 +155,41 @@ struct GeoArgs {
     GeoConst<T> K;
 };
 
+// Everything one slot needs: neighbour differences of u_n (and of u_g when it is a
+// different state), the coefficient row, the reference edge vectors, a's local index.
+template <typename T, int V, bool SAME>
+struct GeoSlot {
+    Vec<T, V> x1[3], x2[3];
+    Vec<T, V> g1[SAME ? 1 : 3], g2[SAME ? 1 : 3];
+    Vec<T, V> c;
+    T e1[3], e2[3];
+    int la;
+};
+
+template <typename T, int V, bool SAME>
+__device__ __forceinline__ void geo_slot_load(GeoSlot<T, V, SAME>& g, const StepArgs<T>& A,
+                                              const GeoArgs<T>& G, int k, size_t S, size_t col,
+                                              const Vec<T, V> (&ua)[3], const Vec<T, V> (&ga)[3]) {
+    const int4 r = __ldg(A.rec + k);
+    g.la = (r.w >> 8) & 3;
+    const size_t o1 = (size_t)r.y * 3 * S + col, o2 = (size_t)r.z * 3 * S + col;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        g.x1[d] = vsub(ldg<T, V>(A.u + o1 + d * S), ua[d]);
+        g.x2[d] = vsub(ldg<T, V>(A.u + o2 + d * S), ua[d]);
+        if constexpr (!SAME) {
+            g.g1[d] = vsub(ldg<T, V>(G.ug + o1 + d * S), ga[d]);
+            g.g2[d] = vsub(ldg<T, V>(G.ug + o2 + d * S), ga[d]);
+        }
+    }
+    g.c = ldg<T, V>(A.coef + (size_t)r.x * S + col);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        g.e1[d] = __ldg(G.geo + (size_t)kGeoStride * k + d);
+        g.e2[d] = __ldg(G.geo + (size_t)kGeoStride * k + 3 + d);
+    }
+}
+
 // One step, rows through L1: per slot the neighbour rows of u_n (and of u_g when it
 // is a different state), the coefficient row and the slot's edge vectors.
 template <typename T, int V, bool SAME>
@@ -184,41 +219,26 @@ __global__ void __launch_bounds__(256) k_step_geo(StepArgs<T> A, GeoArgs<T> G) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) acc[i][d] = load[i][d] = T(0);
     const int k0 = __ldg(A.node_ptr + a), k1 = __ldg(A.node_ptr + a + 1);
+    // The rows, coefficient and edge vectors of slot k+1 are requested before slot k is
+    // formed (one slot of lookahead; the per-slot geometry hides their latency).
+    GeoSlot<T, V, SAME> nx;
+    if (k0 < k1) geo_slot_load<T, V, SAME>(nx, A, G, k0, S, col, ua, ga);
     for (int k = k0; k < k1; ++k) {
-        const int4 r = __ldg(A.rec + k);
-        const int la = (r.w >> 8) & 3;
-        const size_t o1 = (size_t)r.y * 3 * S + col, o2 = (size_t)r.z * 3 * S + col;
-        Vec<T, V> x1[3], x2[3], g1[3], g2[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            x1[d] = vsub(ldg<T, V>(A.u + o1 + d * S), ua[d]);
-            x2[d] = vsub(ldg<T, V>(A.u + o2 + d * S), ua[d]);
-            if constexpr (SAME) {
-                g1[d] = x1[d];
-                g2[d] = x2[d];
-            } else {
-                g1[d] = vsub(ldg<T, V>(G.ug + o1 + d * S), ga[d]);
-                g2[d] = vsub(ldg<T, V>(G.ug + o2 + d * S), ga[d]);
-            }
-        }
-        const Vec<T, V> c = ldg<T, V>(A.coef + (size_t)r.x * S + col);
-        T e1[3], e2[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            e1[d] = __ldg(G.geo + (size_t)kGeoStride * k + d);
-            e2[d] = __ldg(G.geo + (size_t)kGeoStride * k + 3 + d);
-        }
+        const GeoSlot<T, V, SAME> cu = nx;
+        if (k + 1 < k1) geo_slot_load<T, V, SAME>(nx, A, G, k + 1, S, col, ua, ga);
 #pragma unroll
         for (int i = 0; i < V; ++i) {
             T q1[3], q2[3], d1[3], d2[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                q1[d] = e1[d] + g1[d].v[i];
-                q2[d] = e2[d] + g2[d].v[i];
-                d1[d] = x1[d].v[i];
-                d2[d] = x2[d].v[i];
+                const T g1 = SAME ? cu.x1[d].v[i] : cu.g1[d].v[i];
+                const T g2 = SAME ? cu.x2[d].v[i] : cu.g2[d].v[i];
+                q1[d] = cu.e1[d] + g1;
+                q2[d] = cu.e2[d] + g2;
+                d1[d] = cu.x1[d].v[i];
+                d2[d] = cu.x2[d].v[i];
             }
-            geo_row<T>(la, q1, q2, d1, d2, c.v[i], G.K, acc[i], load[i]);
+            geo_row<T>(cu.la, q1, q2, d1, d2, cu.c.v[i], G.K, acc[i], load[i]);
         }
     }
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
@@ -236,6 +256,14 @@ __global__ void __launch_bounds__(256) k_step_geo(StepArgs<T> A, GeoArgs<T> G) {
         stcs<T, V>(A.un + row + d * S, o);
     }
 }
+
+struct GeoTuning {
+    int vec;    // samples per thread (upper bound)
+    int block;  // threads per block (64, 128 or 256)
+};
+// Defaults from sweeps on the 256x1024 tube, 512 samples (B200).
+static GeoTuning g_geo32 = {4, 128};
+static GeoTuning g_geo64 = {1, 128};
 
 template <typename T>
 int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* geo,
@@ -280,23 +308,30 @@ int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, con
     G.K.inv4pe3 = (T)(0.25 / (1.0 - nu * nu));
     const bool same = G.ug == u;
     const void* ptrs[6] = {coef, invm, u, up, un, G.ug};
+    const GeoTuning& tu = sizeof(T) == 4 ? g_geo32 : g_geo64;
     int V = (int)(16 / sizeof(T));
-    if (V > 2) V = 2;
+    while (V > tu.vec) V /= 2;
     for (; V > 1; V /= 2) {
         bool ok = A.S % V == 0;
         for (int i = 0; i < 6; ++i)
             if (reinterpret_cast<uintptr_t>(ptrs[i]) % (V * sizeof(T))) ok = false;
         if (ok) break;
     }
-    const RowGrid rg = row_grid(m->n_nodes, A.S / V, 128);
+    const int block = tu.block;
+    const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
     A.tpn = rg.tpn;
     A.npb = rg.npb;
-    if (V == 2) {
-        if (same) k_step_geo<T, 2, true><<<rg.grid, 128, 0, st>>>(A, G);
-        else k_step_geo<T, 2, false><<<rg.grid, 128, 0, st>>>(A, G);
+    if (V == 4) {
+        if constexpr (sizeof(T) == 4) {
+            if (same) k_step_geo<T, 4, true><<<rg.grid, block, 0, st>>>(A, G);
+            else k_step_geo<T, 4, false><<<rg.grid, block, 0, st>>>(A, G);
+        }
+    } else if (V == 2) {
+        if (same) k_step_geo<T, 2, true><<<rg.grid, block, 0, st>>>(A, G);
+        else k_step_geo<T, 2, false><<<rg.grid, block, 0, st>>>(A, G);
     } else {
-        if (same) k_step_geo<T, 1, true><<<rg.grid, 128, 0, st>>>(A, G);
-        else k_step_geo<T, 1, false><<<rg.grid, 128, 0, st>>>(A, G);
+        if (same) k_step_geo<T, 1, true><<<rg.grid, block, 0, st>>>(A, G);
+        else k_step_geo<T, 1, false><<<rg.grid, block, 0, st>>>(A, G);
     }
     CVFES_LAUNCH_CHECK("k_step_geo");
     return CVFES_OK;
@@ -354,6 +389,24 @@ int launch_advance_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, 
 }  // namespace cvfes
 
 using namespace cvfes;
+
+extern "C" int cvfes_set_geo_tuning(int32_t precision, int32_t vec, int32_t block) {
+    if ((precision != 32 && precision != 64) || (vec != 1 && vec != 2 && vec != 4) ||
+        (precision == 64 && vec == 4) || (block != 64 && block != 128 && block != 256))
+        return fail(CVFES_ERR_ARG, "cvfes_set_geo_tuning: bad argument");
+    GeoTuning& t = precision == 32 ? g_geo32 : g_geo64;
+    t = GeoTuning{vec, block};
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_get_geo_tuning(int32_t precision, int32_t* vec, int32_t* block) {
+    if (precision != 32 && precision != 64)
+        return fail(CVFES_ERR_ARG, "cvfes_get_geo_tuning: precision must be 32 or 64");
+    const GeoTuning& t = precision == 32 ? g_geo32 : g_geo64;
+    if (vec) *vec = t.vec;
+    if (block) *block = t.block;
+    return CVFES_OK;
+}
 
 extern "C" int cvfes_solid_slot_geometry_f64(int64_t n_elems, const double* nodes,
                                              const int32_t* elems, const int32_t* slot_rec,

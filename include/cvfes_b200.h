@@ -354,6 +354,10 @@ int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, const int
  * cvfes_solid_slot_geometry_f64 (nodes device f64 [N][3], elems device int32 [E][3]).
  * ug: geometry displacement [3N][S] (NULL or == u: the current state).
  * nu: Poisson ratio of D (physicsSolver.py:184-188, shear factor 5/6).          */
+/* Geometric-step kernel choice per precision: samples per thread (1|2|4, FP64 1|2) and
+ * threads per block (64|128|256); every choice gives bitwise the same results. */
+int cvfes_set_geo_tuning(int32_t precision, int32_t vec, int32_t block);
+int cvfes_get_geo_tuning(int32_t precision, int32_t* vec, int32_t* block);
 int cvfes_solid_slot_geometry_f64(int64_t n_elems, const double* nodes, const int32_t* elems,
                                   const int32_t* slot_rec, double* geo64, float* geo32,
                                   void* stream);

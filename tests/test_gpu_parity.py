@@ -450,3 +450,28 @@ def test_tiled_step_with_outliers_matches_fan(lib, cuda, precision):
     finally:
         _lib.set_step_tuning(precision, **saved)
     assert torch.equal(s.local_displacement(), ref.local_displacement())
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_geometric_step_tunings_are_bitwise_identical(lib, cuda, precision):
+    """Samples per thread and block size of the geometric step change no bits."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(64)
+    pres = case.pressures(24) * 5.0
+    saved = [C_int() for C_int in (_lib.C.c_int32, _lib.C.c_int32)]
+    call("cvfes_get_geo_tuning", precision, _lib.C.byref(saved[0]), _lib.C.byref(saved[1]))
+    outs = []
+    try:
+        for vec, block in ([(1, 64), (2, 128), (4, 256), (4, 128)] if precision == 32
+                           else [(1, 64), (2, 128), (2, 256)]):
+            call("cvfes_set_geo_tuning", precision, vec, block)
+            cfg = Cfg(case.dt, 64, precision, chunk=12)
+            cfg.update_interval = 1
+            s = GPUSolidSolver(LocalComm(), mesh, cfg)
+            s.Advance(pres)
+            outs.append(s.local_displacement().clone())
+    finally:
+        call("cvfes_set_geo_tuning", precision, saved[0].value, saved[1].value)
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
