@@ -185,10 +185,8 @@ def run_gpu(args):
                                 device_id=dev)
     case = CASES[args.workload]
     prec = 32 if args.precision == "fp32" else 64
-    import dataclasses
-    rcase = dataclasses.replace(case, seed_E=case.seed_E + 1000 * rank,
-                                seed_h=case.seed_h + 1000 * rank)
-    mesh = build_mesh(rcase)
+    from cvfes_b200.replicas import max_over_ranks, rank_case
+    mesh = build_mesh(rank_case(case, rank))
     S, N, E = mesh.nSmp, mesh.nNodes, mesh.nElements
 
     class Cfg:
@@ -231,10 +229,7 @@ def run_gpu(args):
     ms = ev0.elapsed_time(ev1)
     clocks.stop()
     ck = clocks.summary(t_wall0, t_wall1)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, dev)
     chunk = args.chunk
     launches = K + K // chunk + (1 if K % chunk else 0)
 
@@ -272,9 +267,8 @@ def run_gpu(args):
         stream.synchronize()
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    ms2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    ms2 = max_over_ranks(e0.elapsed_time(e1), dev)
     if world > 1:
-        dist.all_reduce(ms2, op=dist.ReduceOp.MAX)
         dist.barrier()
     solver.release_graphs()
 
@@ -305,7 +299,7 @@ def run_gpu(args):
                        "dt": Cfg.dt, "parallelism": f"replicas{world}",
                        "l2": "state 3x%.2f GB > L2, no flush" % (3 * N * S * b / 1e9),
                        "graph_chunk": chunk, "finite": finite},
-            "e2e": {"value": world * S * K2 / (float(ms2.item()) * 1e-3), "unit": UNIT,
+            "e2e": {"value": world * S * K2 / (ms2 * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": 8, "d2h_bytes_per_step": S * 4 * 8},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
@@ -346,10 +340,8 @@ def run_adjoint(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
     prec = 32 if args.precision == "fp32" else 64
-    import dataclasses
-    rcase = dataclasses.replace(case, seed_E=case.seed_E + 1000 * rank,
-                                seed_h=case.seed_h + 1000 * rank)
-    problem, logE, logh, _ = adjoint_setup(rcase, precision=prec, device=dev)
+    from cvfes_b200.replicas import max_over_ranks, rank_case
+    problem, logE, logh, _ = adjoint_setup(rank_case(case, rank), precision=prec, device=dev)
     S, N, E, T = problem.S, problem.N, problem.E, problem.T
     log_h = problem.grad_logh
     logE_d, logh_d = logE.to(dev), logh.to(dev)
@@ -376,10 +368,7 @@ def run_adjoint(args):
     clocks.stop()
     fwd = sum(evs[3 * k].elapsed_time(evs[3 * k + 1]) for k in range(K))
     adj = sum(evs[3 * k + 1].elapsed_time(evs[3 * k + 2]) for k in range(K))
-    tot = torch.tensor([fwd + adj, fwd, adj], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    ms_tot, ms_fwd, ms_adj = (float(x) for x in tot.cpu())
+    ms_tot, ms_fwd, ms_adj = (max_over_ranks(x, dev) for x in (fwd + adj, fwd, adj))
     finite = bool(torch.isfinite(problem.J).all())
 
     # e2e through the autograd.Function with host tensors in and gradients out
@@ -492,10 +481,8 @@ def run_batched(args):
     t1 = time.perf_counter()
     clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    from cvfes_b200.replicas import max_over_ranks
+    ms_max = max_over_ranks(ms, dev)
     finite = all(bool(np.all(n[:, 3] == 0)) for n in batch.Norms(check_finite=False))
     S_total = batch.sample_count()
     bstep = batch.algorithmic_bytes()
