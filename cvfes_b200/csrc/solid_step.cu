@@ -1193,6 +1193,15 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     int V = pick_vec<T>(ptrs, 5, A.S);
     while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
+    // The warp-per-node kernels need S/V to be a multiple of 32: narrow the sample
+    // vector to make it so (S = 64 with 4 per thread -> 2 per thread), else they fall
+    // back to the row-gather kernel at the original width.
+    const int V_rows = V;
+    if (tune.staged != 0 && (A.S / V) % 32 != 0) {
+        int v2 = V;
+        while (v2 > 1 && (A.S / v2) % 32 != 0) v2 /= 2;
+        if ((A.S / v2) % 32 == 0) V = v2;
+    }
     if (tune.staged == 7) {  // TMA-tiled strips; the fan kernel where they do not apply
         const int trc = launch_step_tile<T>(m, A, tune.vec, st);
         if (trc <= 0) return trc;
@@ -1243,6 +1252,7 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
         }
         return rc;
     }
+    V = V_rows;
     const int block = 256;
     const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
     A.tpn = rg.tpn;
