@@ -40,6 +40,7 @@ struct StepArgs {
     int gather_rows; // rows of each warp's gather buffer (gather kernel)
     int nch;         // sample chunks per node block (staged kernels; 1D grid, chunk fastest)
     int* status;     // bit 0: a bounded wait gave up
+    int pf_dist = 0; // fan kernel: nodes ahead whose rows are prefetched into L2 (0: off)
 };
 
 // ------------------------------------------------------------ TMA / mbarrier helpers
@@ -82,6 +83,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase, 
 }
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+// L2 prefetch of a byte range by the bulk-copy unit (no registers, no L1 line).  The
+// range is shrunk to 16-byte boundaries, so nothing outside [p, p + bytes) is touched.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, size_t bytes) {
+    uintptr_t b = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    while (b < e) {
+        const uint32_t n = (uint32_t)((e - b) < 32768 ? (e - b) : 32768);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"(n) : "memory");
+        b += n;
+    }
 }
 constexpr int kMaxPolls = 1 << 22;
 

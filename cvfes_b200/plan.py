@@ -99,6 +99,9 @@ class SolidPlan:
         node_ptr, slot_rec, elem_slot = incidence(elements, self.N)
         self.host_node_ptr, self.host_slot_rec = node_ptr, slot_rec
         self.max_degree = int(np.max(np.diff(node_ptr))) if self.N > 0 else 0
+        # node-numbering bandwidth: how far ahead of a node its neighbours' rows lie
+        self.bandwidth = int(np.max(elements.max(axis=1) - elements.min(axis=1))) \
+            if self.E > 0 else 0
         dev = self.device
         self.stream = torch.cuda.current_stream(dev)
         self.nodes = torch.from_numpy(nodes).to(dev)
@@ -193,6 +196,7 @@ class SolidPlan:
         d = _lib.SolidMeshDesc(self.N, self.E, self.S, self.n_clamped, self.clamp_value,
                                ptr(self.node_ptr), ptr(self.slot_rec), ptr(slab), ptr(fhat),
                                self.max_degree, ptr(self.status))
+        d.bandwidth = self.bandwidth
         if getattr(self, "tile_win", None) is not None:
             P, H, W, EH, WE = self.tile_shape
             d.tile_win, d.tile_rec, d.node_loc = (ptr(self.tile_win), ptr(self.tile_rec),

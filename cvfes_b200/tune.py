@@ -1,7 +1,8 @@
 """Autotuner for the step kernels: measure candidate tile shapes, keep the fastest.
 
 Single mesh: the kernel variant, samples per thread (VEC), nodes per block and
-the register bound (``cvfes_set_step_tuning``).  Batch: samples per thread (the
+the register bound (``cvfes_set_step_tuning``), then the fan kernel's L2 prefetch
+distance (``cvfes_set_step_prefetch``).  Batch: samples per thread (the
 tile's sample width, 32*VEC per warp) and the persistent grid size.  Every
 candidate runs a few CUDA-graph chunks from the same saved state, timed with CUDA
 events; the state is restored afterwards, so tuning does not advance the
@@ -78,29 +79,46 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
     if key in cache:
         best = cache[key]
         _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
+        _lib.set_step_prefetch(prec, best.get("prefetch", -1))
         return dict(best, cached=True)
     saved = [b.clone() for b in solver.bufs]
     roles = (solver.cur, solver.prev, solver.nxt)
     pres = np.zeros(steps + solver.graph_chunk)
+
+    def measure():
+        solver.release_graphs()
+        for b, s in zip(solver.bufs, saved):
+            b.copy_(s)
+        solver.cur, solver.prev, solver.nxt = roles
+        solver.Advance(pres[:solver.graph_chunk])  # capture + warm
+        return _time_ms(lambda: solver.Advance(pres[:steps]), dev) / steps
+
+    # tile shapes with the automatic L2 prefetch distance, then the distance for the
+    # fastest shape (fan kernel only): off, automatic, twice the mesh bandwidth
+    _lib.set_step_prefetch(prec, -1)
     results = []
     for staged, vec, npb, minb in (candidates or STEP_CANDIDATES[prec]):
         try:
             _lib.set_step_tuning(prec, vec, npb, staged, minb)
         except _lib.CvfesError:
             continue
-        solver.release_graphs()
-        for b, s in zip(solver.bufs, saved):
-            b.copy_(s)
-        solver.cur, solver.prev, solver.nxt = roles
-        solver.Advance(pres[:solver.graph_chunk])  # capture + warm
-        ms = _time_ms(lambda: solver.Advance(pres[:steps]), dev) / steps
-        results.append((ms, dict(staged=staged, vec=vec, npb=npb, minb=minb, ms_per_step=ms)))
+        ms = measure()
+        results.append((ms, dict(staged=staged, vec=vec, npb=npb, minb=minb, prefetch=-1,
+                                 ms_per_step=ms)))
+    best = min(results, key=lambda r: r[0])[1]
+    _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
+    if best["staged"] == 3:
+        for dist in (0, 2 * solver.plan.bandwidth + 128):
+            _lib.set_step_prefetch(prec, dist)
+            ms = measure()
+            results.append((ms, dict(best, prefetch=dist, ms_per_step=ms)))
+        best = min(results, key=lambda r: r[0])[1]
+    _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
+    _lib.set_step_prefetch(prec, best["prefetch"])
     for b, s in zip(solver.bufs, saved):
         b.copy_(s)
     solver.cur, solver.prev, solver.nxt = roles
     solver.release_graphs()
-    best = min(results, key=lambda r: r[0])[1]
-    _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
     if use_cache:
         _store(key, best)
     return dict(best, cached=False, tried=[r[1] for r in results])

@@ -32,3 +32,23 @@ def test_version_and_error_channel(lib):
     rc = lib.cvfes_mesh_incidence(0, 0, None, None, None, None)
     assert rc == _lib.CVFES_ERR_ARG
     assert "cvfes_mesh_incidence" in _lib.last_error()
+
+
+def test_tuning_setters_validate_and_round_trip(lib):
+    """Host-only tuning knobs: arguments are checked, values read back."""
+    saved = _lib.get_step_prefetch(32)
+    try:
+        _lib.set_step_prefetch(32, 300)
+        assert _lib.get_step_prefetch(32) == 300
+        for bad in ((32, -2), (32, (1 << 20) + 1), (16, 4)):
+            assert lib.cvfes_set_step_prefetch(*bad) == _lib.CVFES_ERR_ARG
+            assert "cvfes_set_step_prefetch" in _lib.last_error()
+        assert _lib.get_step_prefetch(32) == 300
+        _lib.set_step_prefetch(32, -1)  # automatic: from the mesh's bandwidth
+        assert _lib.get_step_prefetch(32) == -1
+    finally:
+        _lib.set_step_prefetch(32, saved)
+    t = _lib.get_step_tuning(64)
+    assert lib.cvfes_set_step_tuning(64, 4, 2, 3, 2) == _lib.CVFES_ERR_ARG  # FP64 vec <= 2
+    assert lib.cvfes_set_step_tuning(32, 4, 2, 8, 2) == _lib.CVFES_ERR_ARG  # no variant 8
+    assert _lib.get_step_tuning(64) == t

@@ -97,11 +97,13 @@ def test_step_tuner_picks_a_variant(lib, cuda, tmp_path, monkeypatch):
     case = CASES["tube64x128"]
     mesh = build_mesh(case, n_samples=128)
     s = GPUSolidSolver(LocalComm(), mesh, _Cfg(case.dt, 128, 32))
-    saved = _lib.get_step_tuning(32)
+    saved, saved_pf = _lib.get_step_tuning(32), _lib.get_step_prefetch(32)
     try:
         before = s.local_displacement().clone()
         best = tune_step(s, steps=24)
         assert torch.equal(before, s.local_displacement())
         assert best["ms_per_step"] > 0 and _lib.get_step_tuning(32)["staged"] == best["staged"]
+        assert _lib.get_step_prefetch(32) == best["prefetch"]
     finally:
         _lib.set_step_tuning(32, **saved)
+        _lib.set_step_prefetch(32, saved_pf)

@@ -302,6 +302,32 @@ def test_burst_step_variant_matches_fan(lib, cuda):
             assert torch.equal(o, outs[0])
 
 
+def test_fan_prefetch_distance_leaves_results_unchanged(lib, cuda):
+    """L2 prefetch of the nodes ahead (1, 80, the automatic distance and past the mesh
+    end) gives the fan kernel's bits with prefetch off (FP32 and FP64)."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    pres = case.pressures(36)
+    for precision, S, vec in ((32, 128, 4), (64, 64, 2)):
+        mesh = c0_mesh(S)
+        saved, saved_pf = _lib.get_step_tuning(precision), _lib.get_step_prefetch(precision)
+        outs = []
+        try:
+            _lib.set_step_tuning(precision, vec, 2, 3, 2)
+            for dist in (0, 1, 80, -1, 1 << 20):
+                _lib.set_step_prefetch(precision, dist)
+                s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+                s.Advance(pres)
+                s.plan.check_status()
+                outs.append(s.local_displacement().clone())
+                s.release_graphs()
+        finally:
+            _lib.set_step_tuning(precision, **saved)
+            _lib.set_step_prefetch(precision, saved_pf)
+        for o in outs[1:]:
+            assert torch.equal(o, outs[0])
+
+
 @pytest.mark.parametrize("name", ["tube8x6_geo1.npz", "tube8x6_geo3.npz"])
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("path", ["solve", "advance"])
