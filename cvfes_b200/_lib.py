@@ -134,8 +134,8 @@ SIGNATURES = {
     "cvfes_graph_destroy": (C.c_int, [P]),
     "cvfes_set_step_tuning": (C.c_int, [I32, I32, I32, I32, I32]),
     "cvfes_get_step_tuning": (C.c_int, [I32, P, P, P, P]),
-    "cvfes_set_step_prefetch": (C.c_int, [I32, I32]),
-    "cvfes_get_step_prefetch": (C.c_int, [I32, P]),
+    "cvfes_set_step_prefetch": (C.c_int, [I32, I32, I32]),
+    "cvfes_get_step_prefetch": (C.c_int, [I32, P, P]),
     "cvfes_status_read": (C.c_int, [P, P]),
     "cvfes_batch_table_bytes": (C.c_int64, [I32]),
     "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, P]),
@@ -182,14 +182,14 @@ def set_step_tuning(precision: int, vec: int, npb: int, staged: int, minb: int) 
     call("cvfes_set_step_tuning", precision, vec, npb, staged, minb)
 
 
-def get_step_prefetch(precision: int) -> int:
-    v = C.c_int32()
-    call("cvfes_get_step_prefetch", precision, C.byref(v))
-    return v.value
+def get_step_prefetch(precision: int) -> dict:
+    d, p = C.c_int32(), C.c_int32()
+    call("cvfes_get_step_prefetch", precision, C.byref(d), C.byref(p))
+    return dict(distance=d.value, parts=p.value)
 
 
-def set_step_prefetch(precision: int, distance: int) -> None:
-    call("cvfes_set_step_prefetch", precision, distance)
+def set_step_prefetch(precision: int, distance: int = -1, parts: int = -1) -> None:
+    call("cvfes_set_step_prefetch", precision, distance, parts)
 
 
 def get_adjoint_tuning(precision: int) -> dict:

@@ -168,7 +168,39 @@ struct RevArgs {
     int nch;        // sample chunks of 32*VEC per node block (fan kernel)
     int cap_slots;  // slot capacity of the shared-memory stage (fan kernel)
     int* status;    // bit 0: a bounded wait gave up; bit 1: stage too small
+    int pf_dist = 0;   // fan kernel: nodes ahead whose rows are prefetched into L2 (0: off)
+    int pf_parts = 0;  // bit 0: node rows; bit 1: element coefficient and Gamma rows
+    int pf_group = 1;  // node blocks covered by one prefetching block
 };
+
+// Prefetch into L2 the rows that nodes a0 .. a0 + n - 1 read in a reverse step: u_n,
+// chi_{n+1}, u_{n+1}, chi_{n+2}, inverse mass, the G row, and the coefficient and
+// Gamma rows of their elements (found through their slot records).
+template <typename T, bool GM>
+__device__ __forceinline__ void rev_prefetch(const RevArgs<T>& A, long long a0, int n,
+                                             int lane) {
+    if (a0 >= A.n_nodes) return;
+    const long long a1 = (a0 + n < A.n_nodes) ? a0 + n : A.n_nodes;
+    const size_t S = (size_t)A.S;
+    const size_t nrow = (size_t)(a1 - a0) * S * sizeof(T);
+    if (A.pf_parts & 1) {
+        if (lane == 0) bulk_prefetch_l2(A.u + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 1) bulk_prefetch_l2(A.x + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 2) bulk_prefetch_l2(A.uo + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 3) bulk_prefetch_l2(A.xo + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 4) bulk_prefetch_l2(A.invm + (size_t)a0 * S, nrow);
+        if constexpr (GM) {
+            if (lane == 5) bulk_prefetch_l2(A.gm + (size_t)a0 * S, nrow);
+        }
+    }
+    if (!(A.pf_parts & 2)) return;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    for (int k = kb + lane; k < ke; k += 32) {
+        const size_t e = (size_t)__ldg(&A.rec[k].x);
+        bulk_prefetch_l2(A.coef + e * S, S * sizeof(T));
+        bulk_prefetch_l2(A.gam + e * S, S * sizeof(T));
+    }
+}
 
 template <typename T>
 __device__ __forceinline__ void load27(const T* K, T (&kk)[27]) {
@@ -535,6 +567,8 @@ __global__ void __launch_bounds__(256, MINB) k_reverse_fan(RevArgs<T> A) {
         }
         prefetch_l2(A.invm + (size_t)a * S + col);
     }
+    if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
+        rev_prefetch<T, GM>(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
     if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
         if (lane == 0 && A.status) atomicOr(A.status, 1);
         return;
@@ -689,6 +723,9 @@ int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T*
     A.inv1meta = (T)(1.0 / (1.0 - eta));
     A.w0 = (T)(d->dt * d->dt / (1.0 + g));
     const RevTuning tu = rev_tuning<T>();
+    const Prefetch pf = step_prefetch(sizeof(T) == 4 ? 32 : 64, m->bandwidth);
+    A.pf_dist = pf.dist;
+    A.pf_parts = pf.parts;
     const void* ptrs[8] = {d->coef, d->invm, u, uo, x, xo, d->gamma, d->gmass};
     int V = (int)(16 / sizeof(T));
     while (V > tu.vec) V /= 2;
@@ -712,6 +749,8 @@ int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T*
         A.npb = tu.npb;
         A.tpn = 32;
         A.nch = A.S / V / 32;
+        A.pf_group = prefetch_group(A.nch);
+        A.pf_parts = prefetch_parts(A.pf_parts, A.nch);
         A.cap_slots = (int)cap;
         fan_grid = (unsigned)(((m->n_nodes + A.npb - 1) / A.npb) * A.nch);
     }

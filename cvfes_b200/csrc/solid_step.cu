@@ -266,28 +266,10 @@ __global__ void k_bsr_spmv(long long n_nodes, int S, const long long* __restrict
 __global__ void k_clock_add(long long* clock, long long n) { clock[0] += n; }
 
 // ------------------------------------------------------------ fan-rotation step
-// Prefetch into L2 the rows that nodes a0 .. a0 + npb - 1 will read: their displacement
-// rows (which lower-numbered neighbours touch first), previous displacement, inverse
-// mass and the coefficient rows of their elements.  One lane per contiguous range; the
-// coefficient rows are found through the nodes' slot records.
-template <typename T>
-__device__ __forceinline__ void fan_prefetch(const StepArgs<T>& A, long long a0, int lane) {
-    if (a0 >= A.n_nodes) return;
-    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
-    const size_t S = (size_t)A.S;
-    const size_t nrow = (size_t)(a1 - a0) * S * sizeof(T);
-    if (lane == 0) bulk_prefetch_l2(A.u + (size_t)a0 * 3 * S, 3 * nrow);
-    if (lane == 1) bulk_prefetch_l2(A.up + (size_t)a0 * 3 * S, 3 * nrow);
-    if (lane == 2) bulk_prefetch_l2(A.invm + (size_t)a0 * S, nrow);
-    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
-    for (int k = kb + lane; k < ke; k += 32)
-        bulk_prefetch_l2(A.coef + (size_t)__ldg(&A.rec[k].x) * S, S * sizeof(T));
-}
-
 // TMA-staged slot rows (as k_step_staged) + the fan-rotation row; 1D grid with the
 // sample chunk fastest, so the chunks of one node block share its slot rows in L2.
-// With pf_dist > 0 the last warp of each node block's first chunk prefetches the rows
-// of the nodes pf_dist ahead.
+// With pf_dist > 0 the last warp of the first chunk of every pf_group-th node block
+// prefetches the rows of the pf_group node blocks pf_dist nodes ahead.
 template <typename T, int V, bool DIFF, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -334,7 +316,8 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
         prefetch_l2(A.invm + (size_t)a * S + col);
         node_load<T>(A, a, step_pressure<T>(A), f);
     }
-    if (A.pf_dist > 0 && chunk == 0 && warp == A.npb - 1) fan_prefetch(A, a0 + A.pf_dist, lane);
+    if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
+        fan_prefetch(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
     if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
         if (lane == 0 && A.status) atomicOr(A.status, 1);
         return;
@@ -1026,17 +1009,24 @@ struct StepTuning {
 // kernel, 2 nodes per block, 2 blocks per SM worth of registers.
 static StepTuning g_tune32 = {4, 2, 3, 2};
 static StepTuning g_tune64 = {2, 2, 3, 2};
-// L2 prefetch distance of the fan kernel in nodes (-1: the mesh's bandwidth + 128;
-// 0: off).  Sweeps on the 256x1024 tube (bandwidth 257, 512 samples): 256 .. 768
-// nodes ahead are equally good (FP32 -3.3%, FP64 -4.2% step time); 2048 and more
-// overflow what L2 keeps and are slower than none.
-static int g_pf32 = -1;
-static int g_pf64 = -1;
-inline int prefetch_nodes(int knob, long long bandwidth) {
-    if (knob >= 0) return knob;
-    if (bandwidth <= 0) return 0;
-    const long long d = bandwidth + 128;
-    return d < (1 << 20) ? (int)d : (1 << 20);
+// L2 prefetch of the fan kernels: distance in nodes (-1: the mesh's bandwidth + 128;
+// 0: off) and parts (bit 0 node rows, bit 1 element coefficient rows; -1: automatic).
+// Sweeps on the 256x1024 tube (bandwidth 257, 512 samples): 256 .. 768 nodes ahead
+// are equally good (FP32 -3%, FP64 -3.5% step time with both parts, none with node
+// rows alone); 2048 and more overflow what L2 keeps and are slower than none.  On the
+// stenosed 512x2048 tube (128 samples) both parts slow the forward step by 4.5% and
+// node rows alone speed the reverse step up by 2.4%.
+static int g_pf_dist[2] = {-1, -1};
+static int g_pf_parts[2] = {-1, -1};
+Prefetch step_prefetch(int precision, long long bandwidth) {
+    const int q = precision == 32 ? 0 : 1;
+    Prefetch p{g_pf_dist[q], g_pf_parts[q]};
+    if (p.dist < 0) {
+        const long long d = bandwidth > 0 ? bandwidth + 128 : 0;
+        p.dist = d < (1 << 20) ? (int)d : (1 << 20);
+    }
+    if (p.parts == 0) p.dist = 0;
+    return p;
 }
 template <typename T>
 StepTuning& tuning_of() {
@@ -1223,7 +1213,9 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     A.cap_slots = 0;
     const void* ptrs[6] = {coef, invm, u, up, un, nullptr};
     StepTuning tune = tuning_of<T>();
-    A.pf_dist = prefetch_nodes(sizeof(T) == 4 ? g_pf32 : g_pf64, m->bandwidth);
+    const Prefetch pf = step_prefetch(sizeof(T) == 4 ? 32 : 64, m->bandwidth);
+    A.pf_dist = pf.dist;
+    A.pf_parts = pf.parts;
     int V = pick_vec<T>(ptrs, 5, A.S);
     while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
@@ -1271,6 +1263,8 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
         A.tpn = 32;
         A.cap_slots = (int)cap;
         A.nch = A.S / V / 32;
+        A.pf_group = prefetch_group(A.nch);
+        A.pf_parts = prefetch_parts(A.pf_parts, A.nch);
         const dim3 grid((unsigned)((m->n_nodes + A.npb - 1) / A.npb), (unsigned)(A.S / V / 32));
         const int threads = 32 * A.npb;
         if (V == 4) {
@@ -1600,19 +1594,25 @@ extern "C" int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* n
     return CVFES_OK;
 }
 
-extern "C" int cvfes_set_step_prefetch(int32_t precision, int32_t distance) {
+extern "C" int cvfes_set_step_prefetch(int32_t precision, int32_t distance, int32_t parts) {
     if (precision != 32 && precision != 64)
         return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: precision must be 32 or 64");
     if (distance < -1 || distance > (1 << 20))
         return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: distance must be in -1..2^20");
-    (precision == 32 ? g_pf32 : g_pf64) = distance;
+    if (parts < -1 || parts > 3)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: parts must be in -1..3");
+    const int q = precision == 32 ? 0 : 1;
+    g_pf_dist[q] = distance;
+    g_pf_parts[q] = parts;
     return CVFES_OK;
 }
 
-extern "C" int cvfes_get_step_prefetch(int32_t precision, int32_t* distance) {
+extern "C" int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int32_t* parts) {
     if (precision != 32 && precision != 64)
         return fail(CVFES_ERR_ARG, "cvfes_get_step_prefetch: precision must be 32 or 64");
-    if (distance) *distance = precision == 32 ? g_pf32 : g_pf64;
+    const int q = precision == 32 ? 0 : 1;
+    if (distance) *distance = g_pf_dist[q];
+    if (parts) *parts = g_pf_parts[q];
     return CVFES_OK;
 }
 

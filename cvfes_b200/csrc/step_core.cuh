@@ -40,7 +40,9 @@ struct StepArgs {
     int gather_rows; // rows of each warp's gather buffer (gather kernel)
     int nch;         // sample chunks per node block (staged kernels; 1D grid, chunk fastest)
     int* status;     // bit 0: a bounded wait gave up
-    int pf_dist = 0; // fan kernel: nodes ahead whose rows are prefetched into L2 (0: off)
+    int pf_dist = 0;  // fan kernel: nodes ahead whose rows are prefetched into L2 (0: off)
+    int pf_parts = 0; // bit 0: node rows; bit 1: element coefficient rows
+    int pf_group = 1; // node blocks covered by one prefetching block
 };
 
 // ------------------------------------------------------------ TMA / mbarrier helpers
@@ -110,6 +112,28 @@ __device__ __forceinline__ T* stage_slab(T* base0, size_t stage_bytes, int q) {
     return stage_ptr(base0, stage_bytes, q);
 }
 
+// Prefetch into L2 the rows that nodes a0 .. a0 + n - 1 will read: their displacement
+// rows (which lower-numbered neighbours touch first), previous displacement, inverse
+// mass and the coefficient rows of their elements.  One lane per contiguous range; the
+// coefficient rows are found through the nodes' slot records.
+template <typename T>
+__device__ __forceinline__ void fan_prefetch(const StepArgs<T>& A, long long a0, int n,
+                                             int lane) {
+    if (a0 >= A.n_nodes) return;
+    const long long a1 = (a0 + n < A.n_nodes) ? a0 + n : A.n_nodes;
+    const size_t S = (size_t)A.S;
+    const size_t nrow = (size_t)(a1 - a0) * S * sizeof(T);
+    if (A.pf_parts & 1) {
+        if (lane == 0) bulk_prefetch_l2(A.u + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 1) bulk_prefetch_l2(A.up + (size_t)a0 * 3 * S, 3 * nrow);
+        if (lane == 2) bulk_prefetch_l2(A.invm + (size_t)a0 * S, nrow);
+    }
+    if (!(A.pf_parts & 2)) return;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    for (int k = kb + lane; k < ke; k += 32)
+        bulk_prefetch_l2(A.coef + (size_t)__ldg(&A.rec[k].x) * S, S * sizeof(T));
+}
+
 // Thread -> (node, sample vector).  A block holds `npb` consecutive nodes and
 // `tpn` consecutive sample vectors of each (tpn = min(S/VEC, 32)); blockIdx.y
 // picks the sample chunk, the last one partly filled when S/VEC is not a
@@ -123,6 +147,27 @@ __device__ __forceinline__ bool map_row(int tpn, int npb, long long n_nodes, int
     vec = blockIdx.y * tpn + (threadIdx.x - t * tpn);
     return a < n_nodes && vec < sv;
 }
+
+// L2 prefetch of the fan kernels for a mesh of this bandwidth under the current setting
+// of cvfes_set_step_prefetch: distance in nodes (0: off) and the parts prefetched (bit 0
+// node rows, bit 1 element coefficient rows; -1: by prefetch_parts at launch).
+struct Prefetch {
+    int dist, parts;
+};
+// A prefetching block covers enough node blocks for kPrefetchChunks sample chunks of
+// work (the first chunk of every node block when there are that many chunks), so the
+// per-block cost of issuing the prefetches is spread the same way at any sample count.
+constexpr int kPrefetchChunks = 4;
+inline int prefetch_group(int chunks) {
+    return chunks >= kPrefetchChunks ? 1 : (kPrefetchChunks + chunks - 1) / chunks;
+}
+// Automatic parts (-1): node rows and coefficient rows with at least kPrefetchChunks
+// sample chunks per node block, node rows only below (the coefficient rows' dependent
+// slot-record loads then cost more than they save).
+inline int prefetch_parts(int parts, int chunks) {
+    return parts >= 0 ? parts : (chunks >= kPrefetchChunks ? 3 : 1);
+}
+Prefetch step_prefetch(int precision, long long bandwidth);
 
 struct RowGrid {
     dim3 grid;

@@ -73,6 +73,20 @@ def color_greedy(elements: np.ndarray, n_nodes: int, max_colors: int = 23):
     return colors, n
 
 
+def numbering_bandwidth(elements: np.ndarray, n_clamped: int) -> int:
+    """Largest id distance between two unclamped nodes of one element: how far ahead of
+    a node its neighbours' rows lie (the clamped prefix is left out; its rows are few and
+    read by every end-ring node, so the step kernels keep them cached anyway)."""
+    e = np.asarray(elements, dtype=np.int64)
+    if e.size == 0:
+        return 0
+    free = e >= n_clamped
+    hi = np.where(free, e, -1).max(axis=1)
+    lo = np.where(free, e, np.iinfo(np.int64).max).min(axis=1)
+    ok = hi >= 0
+    return int(np.max(hi[ok] - lo[ok])) if ok.any() else 0
+
+
 class SolidPlan:
     """Mesh-dependent device data of the solid step (one mesh, local numbering).
 
@@ -99,9 +113,7 @@ class SolidPlan:
         node_ptr, slot_rec, elem_slot = incidence(elements, self.N)
         self.host_node_ptr, self.host_slot_rec = node_ptr, slot_rec
         self.max_degree = int(np.max(np.diff(node_ptr))) if self.N > 0 else 0
-        # node-numbering bandwidth: how far ahead of a node its neighbours' rows lie
-        self.bandwidth = int(np.max(elements.max(axis=1) - elements.min(axis=1))) \
-            if self.E > 0 else 0
+        self.bandwidth = numbering_bandwidth(elements, self.n_clamped)
         dev = self.device
         self.stream = torch.cuda.current_stream(dev)
         self.nodes = torch.from_numpy(nodes).to(dev)

@@ -79,7 +79,7 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
     if key in cache:
         best = cache[key]
         _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
-        _lib.set_step_prefetch(prec, best.get("prefetch", -1))
+        _lib.set_step_prefetch(prec, **best.get("prefetch", {}))
         return dict(best, cached=True)
     saved = [b.clone() for b in solver.bufs]
     roles = (solver.cur, solver.prev, solver.nxt)
@@ -93,9 +93,10 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
         solver.Advance(pres[:solver.graph_chunk])  # capture + warm
         return _time_ms(lambda: solver.Advance(pres[:steps]), dev) / steps
 
-    # tile shapes with the automatic L2 prefetch distance, then the distance for the
-    # fastest shape (fan kernel only): off, automatic, twice the mesh bandwidth
-    _lib.set_step_prefetch(prec, -1)
+    # tile shapes with the automatic L2 prefetch, then the prefetch for the fastest
+    # shape (fan kernel only): off, node rows only, both parts, twice as far ahead
+    auto = dict(distance=-1, parts=-1)
+    _lib.set_step_prefetch(prec, **auto)
     results = []
     for staged, vec, npb, minb in (candidates or STEP_CANDIDATES[prec]):
         try:
@@ -103,18 +104,20 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
         except _lib.CvfesError:
             continue
         ms = measure()
-        results.append((ms, dict(staged=staged, vec=vec, npb=npb, minb=minb, prefetch=-1,
+        results.append((ms, dict(staged=staged, vec=vec, npb=npb, minb=minb, prefetch=auto,
                                  ms_per_step=ms)))
     best = min(results, key=lambda r: r[0])[1]
     _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
     if best["staged"] == 3:
-        for dist in (0, 2 * solver.plan.bandwidth + 128):
-            _lib.set_step_prefetch(prec, dist)
+        bw = solver.plan.bandwidth
+        for pf in (dict(distance=0, parts=0), dict(distance=-1, parts=1),
+                   dict(distance=-1, parts=3), dict(distance=2 * bw + 128, parts=3)):
+            _lib.set_step_prefetch(prec, **pf)
             ms = measure()
-            results.append((ms, dict(best, prefetch=dist, ms_per_step=ms)))
+            results.append((ms, dict(best, prefetch=pf, ms_per_step=ms)))
         best = min(results, key=lambda r: r[0])[1]
     _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
-    _lib.set_step_prefetch(prec, best["prefetch"])
+    _lib.set_step_prefetch(prec, **best["prefetch"])
     for b, s in zip(solver.bufs, saved):
         b.copy_(s)
     solver.cur, solver.prev, solver.nxt = roles

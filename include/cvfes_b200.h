@@ -69,9 +69,9 @@ typedef struct cvfes_solid_mesh {
     int32_t        tile_eh;       /* element ids per element window                 */
     int32_t        tile_we;       /* element windows per tile (at most 3)           */
     int32_t        tile_pad;
-    int64_t        bandwidth;     /* max |a - b| over the element edges of the node
-                                     numbering (0: unknown; sets the automatic L2
-                                     prefetch distance of the fan step kernel)     */
+    int64_t        bandwidth;     /* max |a - b| over the element edges between
+                                     unclamped nodes (0: unknown; sets the automatic
+                                     L2 prefetch distance of the fan step kernels) */
 } cvfes_solid_mesh;
 
 /* Step-kernel tuning (the autotuner sets these; defaults: variant 3, FP32 vec 4,
@@ -107,15 +107,21 @@ int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t s
 int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t* staged,
                           int32_t* minb);
 
-/* L2 prefetch distance of the fan-rotation step kernel (staged 3), in nodes:
- * each node block's first sample chunk prefetches into L2, by bulk prefetches, the
- * displacement, previous-displacement, inverse-mass and element-coefficient rows of
- * the nodes `distance` ahead of it.  -1 (default) = automatic: the mesh's bandwidth
- * + 128 nodes (off when the descriptor's bandwidth is 0); 0 = off; else 1..2^20.
+/* L2 prefetch of the fan-rotation step kernel (staged 3) and the fan reverse step:
+ * each node block's first sample chunk prefetches into L2, by bulk prefetches, rows
+ * that the nodes `distance` ahead of it will read.
+ *   distance: in nodes; -1 (default) = the mesh's bandwidth + 128 (off when the
+ *             descriptor's bandwidth is 0); 0 = off; else 1..2^20;
+ *   parts:    bit 0 = the nodes' state, inverse-mass (and adjoint) rows (contiguous
+ *             ranges); bit 1 = the coefficient (and Gamma) rows of their elements,
+ *             found through their slot records; -1 (default) = both with at least 4
+ *             sample chunks per node block, bit 0 alone below.
+ * With fewer than 4 sample chunks per node block only every k-th node block
+ * prefetches, for k node blocks (k = ceil(4 / chunks)).
  * Results are unchanged; only where the loads hit changes.  Applies to launches
- * made after the call.                                                          */
-int cvfes_set_step_prefetch(int32_t precision, int32_t distance);
-int cvfes_get_step_prefetch(int32_t precision, int32_t* distance);
+ * made after the call (graphs keep what they captured).                        */
+int cvfes_set_step_prefetch(int32_t precision, int32_t distance, int32_t parts);
+int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int32_t* parts);
 
 /* Read and clear the device status word of a mesh descriptor (synchronises the
  * stream).  Returns CVFES_ERR_TIMEOUT if a bounded device wait gave up since

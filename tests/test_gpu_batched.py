@@ -106,4 +106,4 @@ def test_step_tuner_picks_a_variant(lib, cuda, tmp_path, monkeypatch):
         assert _lib.get_step_prefetch(32) == best["prefetch"]
     finally:
         _lib.set_step_tuning(32, **saved)
-        _lib.set_step_prefetch(32, saved_pf)
+        _lib.set_step_prefetch(32, **saved_pf)

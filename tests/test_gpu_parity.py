@@ -304,7 +304,8 @@ def test_burst_step_variant_matches_fan(lib, cuda):
 
 def test_fan_prefetch_distance_leaves_results_unchanged(lib, cuda):
     """L2 prefetch of the nodes ahead (1, 80, the automatic distance and past the mesh
-    end) gives the fan kernel's bits with prefetch off (FP32 and FP64)."""
+    end; node rows, coefficient rows or both) gives the fan kernel's bits with prefetch
+    off (FP32 and FP64)."""
     from cvfes_b200.cases import CASES
     case = CASES["tube64x128"]
     pres = case.pressures(36)
@@ -314,8 +315,8 @@ def test_fan_prefetch_distance_leaves_results_unchanged(lib, cuda):
         outs = []
         try:
             _lib.set_step_tuning(precision, vec, 2, 3, 2)
-            for dist in (0, 1, 80, -1, 1 << 20):
-                _lib.set_step_prefetch(precision, dist)
+            for dist, parts in ((0, 0), (1, 3), (80, 1), (80, 2), (-1, -1), (1 << 20, 3)):
+                _lib.set_step_prefetch(precision, dist, parts)
                 s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
                 s.Advance(pres)
                 s.plan.check_status()
@@ -323,7 +324,7 @@ def test_fan_prefetch_distance_leaves_results_unchanged(lib, cuda):
                 s.release_graphs()
         finally:
             _lib.set_step_tuning(precision, **saved)
-            _lib.set_step_prefetch(precision, saved_pf)
+            _lib.set_step_prefetch(precision, **saved_pf)
         for o in outs[1:]:
             assert torch.equal(o, outs[0])
 

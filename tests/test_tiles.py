@@ -71,3 +71,19 @@ def test_bad_arguments_are_rejected(lib):
     from cvfes_b200._lib import CvfesError
     with pytest.raises(CvfesError):
         tiles(np.array([[0, 1, 2]]), 3, 0, 4, 2, 1, 4, 1)  # H < P
+
+
+def test_numbering_bandwidth_leaves_out_the_clamped_prefix():
+    """The solver's numbering puts both end rings first; the bandwidth that sets the L2
+    prefetch distance is that of the unclamped nodes (one ring + 1 on the tube)."""
+    from cvfes_b200.plan import numbering_bandwidth
+    nc, na = 64, 128
+    from cvfes_b200.mesh import TubeGeometry
+    nodes, elems, inl, outl = tube_mesh(TubeGeometry(nc, na, 3.0))
+    boundary = np.concatenate([inl, outl])
+    assert numbering_bandwidth(elems, 0) == nc + 1
+    _, lcl_elems, _, n_clamped = special_assignment(elems, nodes.shape[0], boundary)
+    assert n_clamped == 2 * nc
+    assert numbering_bandwidth(lcl_elems, n_clamped) == nc + 1
+    assert numbering_bandwidth(lcl_elems, 0) > 50 * nc  # the last ring sits in the prefix
+    assert numbering_bandwidth(np.array([[0, 1, 2]]), 3) == 0
