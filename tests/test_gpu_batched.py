@@ -4,7 +4,7 @@ import pytest
 import torch
 
 from cvfes_b200 import _lib
-from cvfes_b200.batched import BatchedSolidSolver
+from cvfes_b200.batched import BatchedSolidSolver, fan_item_nodes
 from cvfes_b200.cases import TubeCase, build_mesh, case_dt
 from cvfes_b200.solver import GPUSolidSolver, LocalComm
 from oracle import solid_oracle as so
@@ -33,15 +33,18 @@ class _Cfg:
 
 
 @pytest.mark.parametrize("precision", [32, 64])
-@pytest.mark.parametrize("variant", [0, 1])
-def test_batch_equals_meshes_advanced_alone(lib, cuda, precision, variant):
+@pytest.mark.parametrize("variant,grouped", [(0, True), (1, True), (1, False)])
+def test_batch_equals_meshes_advanced_alone(lib, cuda, precision, variant, grouped):
     """Row-gather (0) and fan (1) batch kernels, meshes of 16..128 samples (several nodes
-    per warp in the fan layout): the bits of each mesh advanced alone."""
+    per warp in the fan layout), one launch per item shape or one for all: the bits of
+    each mesh advanced alone."""
     cases, meshes, dts = small_batch()
     pres = 1.33e5 * np.minimum(np.arange(100) / 100.0, 1.0)
     batch = BatchedSolidSolver(meshes, dts, precision=precision, device=cuda, graph_chunk=24,
-                               variant=variant)
+                               variant=variant, grouped=grouped)
     assert batch.variant == variant
+    shapes = {fan_item_nodes(m.nSmp, batch.vec) for m in meshes}
+    assert len(batch.groups) == (len(shapes) if grouped else 1)
     batch.Advance(pres[:37], use_graph=True)     # graph chunks + plain remainder
     batch.Advance(pres[37:100], use_graph=True)  # starts at a non-zero rotation
     saved = _lib.get_step_tuning(precision)

@@ -87,3 +87,11 @@ def test_numbering_bandwidth_leaves_out_the_clamped_prefix():
     assert numbering_bandwidth(lcl_elems, n_clamped) == nc + 1
     assert numbering_bandwidth(lcl_elems, 0) > 50 * nc  # the last ring sits in the prefix
     assert numbering_bandwidth(np.array([[0, 1, 2]]), 3) == 0
+
+
+def test_fan_item_shape_of_the_batch_kernel():
+    """Nodes per warp of a batched fan item, the key the batch groups its meshes by."""
+    from cvfes_b200.batched import fan_item_nodes
+    assert [fan_item_nodes(S, 4) for S in (16, 32, 64, 128, 256, 200, 8)] == \
+        [8, 4, 2, 1, 1, 1, 16]
+    assert [fan_item_nodes(S, 1) for S in (16, 32, 64)] == [2, 1, 1]
