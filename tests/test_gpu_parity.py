@@ -257,6 +257,30 @@ def test_large_sample_chunk_against_oracle(lib, cuda):
         assert so.rel_l2(s.displacement(), o.u) < tol
 
 
+def test_full_size_mesh_sample_chunk_against_oracle(lib, cuda):
+    """The 256x1024 tube (262,144 nodes, 523,776 triangles, row-sum mass), a seeded
+    64-sample chunk of its ensemble, 6 steps: the default step kernels (fan rotation
+    with the L2 prefetch) against the oracle's element-template form, FP64 and FP32."""
+    from cvfes_b200.cases import CASES, build_mesh
+    case = CASES["tube256x1024"]
+    mesh = build_mesh(case, n_samples=64)
+    assert case.mass_lumping == "rowsum"  # the reference's lumping with 3x the density
+    coefK, gthick = mesh.element_coefficients()
+    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
+                             3.0 * mesh.density, mesh.v, mesh.damp, case.dt,
+                             backend="template")
+    pres = 1.33e5 * np.arange(6) / 6.0
+    o.run(pres)
+    assert np.linalg.norm(o.u) > 0
+    for precision, tol in ((64, FP64_TOL), (32, FP32_TOL)):
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 64, precision, chunk=3))
+        s.Advance(pres)
+        s.plan.check_status()
+        err = so.rel_l2(s.displacement(), o.u)
+        s.release_graphs()
+        assert err < tol, (precision, err)
+
+
 @pytest.mark.parametrize("S", [200, 72])
 def test_partial_sample_chunks_against_oracle(lib, cuda, S):
     """S/VEC above 32 and not a multiple of 32 (last sample chunk of a node block partly
