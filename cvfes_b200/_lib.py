@@ -148,8 +148,10 @@ SIGNATURES = {
     "cvfes_set_geo_tuning": (C.c_int, [I32, I32, I32]),
     "cvfes_get_geo_tuning": (C.c_int, [I32, P, P]),
     "cvfes_solid_slot_geometry_f64": (C.c_int, [I64, P, P, P, P, P, P]),
-    "cvfes_solid_step_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),
-    "cvfes_solid_step_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, D, D, D, P]),
+    "cvfes_solid_step_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, P, D, D, D,
+                                           P]),
+    "cvfes_solid_step_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, D, P, D, D, D,
+                                           P]),
     "cvfes_solid_advance_geo_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, I64, P, I32,
                                               D, D, D, P, P, P, P]),
     "cvfes_solid_advance_geo_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, P, P, I64, I64, P, I32,

@@ -245,12 +245,16 @@ __global__ void __launch_bounds__(256) k_step_geo(StepArgs<T> A, GeoArgs<T> G) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const Vec<T, V> up = ldcs<T, V>(A.up + row + d * S);
+        // nodal traction (calc_u_appTrac, physicsSolverSDampGPUs.cl:436-446), one per node
+        const T tr = A.trac ? __ldg(A.trac + 4 * a + d) : T(0);
         Vec<T, V> o;
 #pragma unroll
         for (int i = 0; i < V; ++i) {
             const T dv = ua[d].v[i] - up.v[i];
             const T w = A.w0 * im.v[i];
-            const T v = fma(w, p * load[i][d] - acc[i][d], fma(-A.eta, dv, dv));
+            T f = p * load[i][d];
+            if (A.trac) f += tr;
+            const T v = fma(w, f - acc[i][d], fma(-A.eta, dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
         }
         stcs<T, V>(A.un + row + d * S, o);
@@ -268,8 +272,8 @@ static GeoTuning g_geo64 = {1, 128};
 template <typename T>
 int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* geo,
                     const T* u, const T* up, T* un, const T* ug, const double* p_sched,
-                    const long long* clock, long long j, double pressure, double nu, double dt,
-                    double damp, cudaStream_t st) {
+                    const long long* clock, long long j, double pressure, const T* trac,
+                    double nu, double dt, double damp, cudaStream_t st) {
     if (!m || m->n_nodes <= 0 || m->n_samples <= 0 || m->n_samples > INT32_MAX || !m->node_ptr ||
         !m->slot_rec || m->n_clamped < 0 || m->n_clamped > m->n_nodes)
         return fail(CVFES_ERR_ARG, "cvfes_solid_step_geo: incomplete mesh descriptor");
@@ -289,6 +293,7 @@ int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, con
     A.clock = clock;
     A.j = j;
     A.pressure = pressure;
+    A.trac = trac;
     A.n_nodes = m->n_nodes;
     A.S = (int)m->n_samples;
     A.n_clamped = (int)m->n_clamped;
@@ -368,7 +373,7 @@ int launch_advance_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, 
         }
         const T* ug = live ? buf[cur] : ugeo;
         int rc = launch_step_geo<T>(m, coef, invm, geo, buf[cur], buf[prev], buf[nxt], ug, p_sched,
-                                    clock, j, 0.0, nu, dt, damp, st);
+                                    clock, j, 0.0, nullptr, nu, dt, damp, st);
         if (rc) return rc;
         const int old_prev = prev;
         prev = cur;
@@ -425,21 +430,22 @@ extern "C" int cvfes_solid_step_geo_f64(const cvfes_solid_mesh* mesh, const doub
                                         const double* u, const double* up, double* un,
                                         const double* ug, const double* p_sched,
                                         const int64_t* clock, int64_t j, double pressure,
-                                        double nu, double dt, double damp, void* stream) {
+                                        const double* trac, double nu, double dt, double damp,
+                                        void* stream) {
     return launch_step_geo<double>(mesh, coef, invm, slot_geo, u, up, un, ug, p_sched,
-                                   reinterpret_cast<const long long*>(clock), j, pressure, nu, dt,
-                                   damp, (cudaStream_t)stream);
+                                   reinterpret_cast<const long long*>(clock), j, pressure, trac,
+                                   nu, dt, damp, (cudaStream_t)stream);
 }
 
 extern "C" int cvfes_solid_step_geo_f32(const cvfes_solid_mesh* mesh, const float* coef,
                                         const float* invm, const float* slot_geo, const float* u,
                                         const float* up, float* un, const float* ug,
                                         const double* p_sched, const int64_t* clock, int64_t j,
-                                        double pressure, double nu, double dt, double damp,
-                                        void* stream) {
+                                        double pressure, const float* trac, double nu, double dt,
+                                        double damp, void* stream) {
     return launch_step_geo<float>(mesh, coef, invm, slot_geo, u, up, un, ug, p_sched,
-                                  reinterpret_cast<const long long*>(clock), j, pressure, nu, dt,
-                                  damp, (cudaStream_t)stream);
+                                  reinterpret_cast<const long long*>(clock), j, pressure, trac,
+                                  nu, dt, damp, (cudaStream_t)stream);
 }
 
 extern "C" int cvfes_solid_advance_geo_f64(const cvfes_solid_mesh* mesh, const double* coef,

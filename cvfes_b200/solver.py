@@ -15,8 +15,10 @@ Differences by design:
   on the device inside the step kernel, so a step makes no host round trip
   (the reference copies the boundary rows to the host and back every step,
   ``physicsSolverSDampGPUs.py:363-390``);
-* the stiffness is the linear template form: ``K_s = sum_e (E h)_{e,s} Kt_e``
-  assembled once on the undeformed wall (stiffness update interval infinite);
+* the stiffness is the linear template form ``K_s = sum_e (E h)_{e,s} Kt_e``
+  assembled once on the undeformed wall (stiffness update interval 0, the
+  default), or, with ``stiffness_update_interval`` n >= 1, rebuilt matrix-free with
+  the follower pressure on ``x + u`` every n steps (n = 1: ``assemble_K_P``);
 * FP64 (default) or FP32 state, chosen by ``[gpu] precision``.
 """
 from __future__ import annotations
@@ -249,10 +251,8 @@ class GPUSolidSolver(PhysicsSolver):
 
     def _solve_geo(self, dt):
         """One step on the deformed geometry with the reference's update counter
-        (``physicsSolver.py:296-324``; every step for interval 1, as assemble_K_P)."""
-        if self.trac_dev is not None:
-            raise NotImplementedError("nodal traction input is not supported with a "
-                                      "stiffness update interval")
+        (``physicsSolver.py:296-324``; every step for interval 1, as assemble_K_P), with
+        the nodal traction when a traction series drives the wall (calc_u_appTrac)."""
         if self.geo_counter >= self.update_interval:
             if self.update_interval == 1:
                 self.geo_live = True
@@ -266,8 +266,8 @@ class GPUSolidSolver(PhysicsSolver):
         call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
              ptr(self.plan.invm(self.precision)), ptr(self.slot_geo), ptr(self.bufs[self.cur]),
              ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), ptr(ug), None, None, 0,
-             float(self.pressure), float(self.mesh.v), float(dt), float(self.damp),
-             self._stream())
+             float(self.pressure), ptr(self.trac_dev), float(self.mesh.v), float(dt),
+             float(self.damp), self._stream())
 
     def Solve(self, t, dt):
         """One explicit step for all samples (``physicsSolverSDampGPUs.py:325-399``)."""
@@ -299,6 +299,11 @@ class GPUSolidSolver(PhysicsSolver):
         n = int(p.numel())
         prec = self.precision
         if self.update_interval > 0:
+            if self.trac_dev is not None:  # per-step launches with the held traction
+                for j in range(n):
+                    self.pressure = float(pressures[j])
+                    self.Solve(None, dt)
+                return self
             return self._advance_geo(p, n, dt)
         with torch.cuda.device(self.device):
             self.clock.zero_()
@@ -345,9 +350,6 @@ class GPUSolidSolver(PhysicsSolver):
 
     def _advance_geo(self, p, n, dt):
         """Geometric steps as plain launches (the geometry update counter is host state)."""
-        if self.trac_dev is not None:
-            raise NotImplementedError("nodal traction input is not supported with a "
-                                      "stiffness update interval")
         fn = "cvfes_solid_advance_geo_f64" if self.precision == 64 else \
             "cvfes_solid_advance_geo_f32"
         b = self.bufs

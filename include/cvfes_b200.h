@@ -372,6 +372,9 @@ int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, const int
  * slot_geo: [8 * 3E] per slot X_b1 - X_a, X_b2 - X_a (reference coordinates), from
  * cvfes_solid_slot_geometry_f64 (nodes device f64 [N][3], elems device int32 [E][3]).
  * ug: geometry displacement [3N][S] (NULL or == u: the current state).
+ * trac: NULL or the nodal traction [4N] T (x, y, z, pad; local order, clamped rows
+ *       zero), added to the force of every sample as calc_u_appTrac does
+ *       (physicsSolverSDampGPUs.cl:436-446) -- as cvfes_solid_step's trac.
  * nu: Poisson ratio of D (physicsSolver.py:184-188, shear factor 5/6).          */
 /* Geometric-step kernel choice per precision: samples per thread (1|2|4, FP64 1|2) and
  * threads per block (64|128|256); every choice gives bitwise the same results. */
@@ -383,13 +386,14 @@ int cvfes_solid_slot_geometry_f64(int64_t n_elems, const double* nodes, const in
 int cvfes_solid_step_geo_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
                              const double* slot_geo, const double* u, const double* up,
                              double* un, const double* ug, const double* p_sched,
-                             const int64_t* clock, int64_t j, double pressure, double nu,
-                             double dt, double damp, void* stream);
+                             const int64_t* clock, int64_t j, double pressure,
+                             const double* trac, double nu, double dt, double damp,
+                             void* stream);
 int cvfes_solid_step_geo_f32(const cvfes_solid_mesh* mesh, const float* coef, const float* invm,
                              const float* slot_geo, const float* u, const float* up, float* un,
                              const float* ug, const double* p_sched, const int64_t* clock,
-                             int64_t j, double pressure, double nu, double dt, double damp,
-                             void* stream);
+                             int64_t j, double pressure, const float* trac, double nu,
+                             double dt, double damp, void* stream);
 /* n_steps geometric steps with the reference's update counter (physicsSolver.py:299-324):
  * before each step, if *counter >= interval the geometry becomes the current state and
  * *counter = 1, else *counter += 1.  interval 1 reads the geometry straight from u_n

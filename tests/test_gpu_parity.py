@@ -425,10 +425,13 @@ def test_stress_recovery_matches_golden(lib, cuda, name, precision, tmp_path):
     assert saved["u"].shape == (mesh.nSmp, mesh.nNodes, 3)
 
 
+@pytest.mark.parametrize("interval", [0, 1])
 @pytest.mark.parametrize("constant", [False, True])
-def test_traction_series_input_against_oracle(lib, cuda, tmp_path, constant):
+def test_traction_series_input_against_oracle(lib, cuda, tmp_path, constant, interval):
     """Fluid wall traction read from the .npy series of RefreshContext (ramped, then
-    interpolated between files every dt_f; or one constant file), added as nodal force."""
+    interpolated between files every dt_f; or one constant file), added as nodal force,
+    on the undeformed stiffness (interval 0) and with the stiffness and follower pressure
+    rebuilt every step (interval 1: assemble_K_P with calc_u_appTrac)."""
     import math
     g = golden("tube8x6_element.npz")
     mesh = golden_mesh(g)
@@ -445,10 +448,12 @@ def test_traction_series_input_against_oracle(lib, cuda, tmp_path, constant):
     cfg.exportBdyStressFilename = base
     cfg.useConstantStress = constant
     cfg.constant_T, cfg.dt_f, cfg.constant_pressure = 10 * dt, 4 * dt, 5e4
+    cfg.update_interval = interval
     solver = GPUSolidSolver(LocalComm(), mesh, cfg)
     coefK, gthick = mesh.element_coefficients()
     o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
-                             mesh.density, mesh.v, mesh.damp, dt, backend="numpy")
+                             mesh.density, mesh.v, mesh.damp, dt, backend="numpy",
+                             update_interval=interval)
     bdy = (3 * np.asarray(mesh.boundary)[:, None] + np.arange(3)).ravel()
 
     class Clock:
