@@ -488,8 +488,10 @@ def run_batched(args):
     bstep = batch.algorithmic_bytes()
     peaks, peak_kind = measured_peaks()
     achieved = bstep / (ms / K * 1e-3) / 1e9
-    # one step kernel per step, one clock kernel per graph chunk and per plain remainder
-    launches = K + K // batch.graph_chunk + 1
+    # per launch group: one step kernel per step, one clock kernel per graph chunk and
+    # per plain remainder
+    n_groups = len(batch.groups)
+    launches = n_groups * (K + K // batch.graph_chunk + 1)
     if rank == 0:
         line = {
             "metric": METRIC, "value": world * S_total * K / (ms_max * 1e-3), "unit": UNIT,
@@ -502,6 +504,7 @@ def run_batched(args):
                        "parallelism": f"replicas{world}", "kernel": ("fan" if batch.variant == 1
                                                                     else "row gather"),
                        "vec": tuned.get("vec"), "grid": tuned.get("grid"),
+                       "launch_groups": n_groups,
                        "l2": "state > L2, no flush",
                        "finite": finite},
             "gpu_launches": launches,
