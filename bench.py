@@ -2,19 +2,38 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cvfes_b200|reference]
                     [--workload tube256x1024] [--precision fp32|fp64]
+                    [--state auto|previous|velocity] [--legs main,adjoint,batched]
 
 A step is one explicit time step of every sample of the workload.  Default
 workload: the 256 x 1024-node tube (262,144 nodes, 523,776 triangles), 512 GMRF
-samples, dt = 5e-7, FP32 state; K = 2000 steps (the workload's run length).
+samples, dt = 5e-7, FP32 state (velocity-state form); K = 2000 steps (the workload's
+run length).
 
-Metric: sample-timesteps/s = samples x steps / seconds, whole job.  ``value`` is
-measured with CUDA events around the K steps (CUDA-graph replays of the fused
-step kernel) with the state resident in HBM; the state (3 x 1.6 GB) is larger
-than L2, so no flush is needed.  ``e2e`` runs K steps through the public
-per-step API (GPUSolidSolver.Solve with the pressure copied from pinned host
-memory, plus the FP64 watchdog norms read back to pinned host memory every
-step).  Multi-GPU: each rank advances its own independent ensemble (samples do
-not interact), no collectives on the data path; timing is the max over ranks.
+Metric: sample-timesteps/s = samples x steps / seconds, whole job.
+
+* ``value``: CUDA events around ``GPUSolidSolver.Advance`` of the K steps with the
+  state resident in HBM: replays of a captured CUDA graph of ``--chunk`` steps when
+  K >= the chunk, plain launches from one library call for the rest (all of it when
+  K < chunk).  The state (3 x 1.6 GB) is larger than L2, so no flush is needed.
+* ``e2e``: ``--e2e-steps`` steps through the reference's per-step API, as
+  ``TransientSolverGPU`` drives it: ``RefreshContext(fluid)`` (the pressure of time
+  t, passed to the step kernel as a launch argument, 8 bytes) then ``Solve(t, dt)``,
+  then ``Norms(out=pinned)`` -- the FP64 per-sample norms and the non-finite
+  watchdog read back into pinned host memory, which synchronises every step.
+* ``adjoint`` (default line): forward + adjoint gradient evaluations of the
+  64 x 128 tube, 64 samples, 500 steps (FP32 and FP64): gradients/s, the ratio
+  (fwd + adj) / fwd and the reverse pass's bandwidth.
+* ``batched`` (default line): the uneven 64-tube ensemble (FP32) advanced by the
+  batched kernels, sample-timesteps/s summed over the tubes.
+
+``--impl reference`` times the reference's own CPU path of the step (its compiled
+``MultiplyByVector`` plus the NumPy update and Dirichlet rows of
+``physicsSolver.py:263-292``, with ``OMP_NUM_THREADS`` = the host's cores) on a few
+of the workload's samples; its inputs (mesh, the same GMRF sample columns, the same
+mass lumping) come from the oracle's restatement, so the reference arm loads no
+product library.  Multi-GPU: each rank advances its own independent ensemble
+(samples do not interact), no collectives on the data path; timing is the max over
+ranks.
 """
 from __future__ import annotations
 
@@ -44,11 +63,21 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def algorithmic_bytes(N, E, S, b, bt):
+def algorithmic_bytes(N, E, S, b, bt, state="previous"):
     """Bytes one step must move: per sample u_n, u_{n-1} read, u_{n+1} written (9N),
     inverse mass (N), element coefficient (E); shared: int32 connectivity (12 B per
-    element), a 45-entry symmetric template per element and the unit load (3N)."""
-    return S * b * (10 * N + E) + E * (12 + 45 * bt) + 3 * N * bt
+    element), a 45-entry symmetric template per element and the unit load (3N).  The
+    velocity-state form reads u_n and v_n and writes u_{n+1} and v_{n+1} (12N)."""
+    per_node = 13 if state == "velocity" else 10
+    return S * b * (per_node * N + E) + E * (12 + 45 * bt) + 3 * N * bt
+
+
+def adjoint_bytes(N, E, S, b, bt, log_h):
+    """Bytes one reverse step must move: per sample u_n, u_{n+1} read and u_{n-1}
+    written (backward reconstruction, 9N), chi_{n+1}, chi_{n+2} read and chi_n written
+    (9N), inverse mass (N), coefficient (E), the Gamma accumulator read and written
+    (2E) and, for log h, the G accumulator (2N); shared data as in the forward step."""
+    return S * b * (19 * N + 3 * E + (2 * N if log_h else 0)) + E * (12 + 45 * bt) + 3 * N * bt
 
 
 class ClockSampler:
@@ -119,19 +148,46 @@ def dist_setup(args):
     return rank, world, local
 
 
+def workload_config(args, case, world):
+    """The workload description both arms print (the same dict, key for key)."""
+    N, E = case.nc * case.na, 2 * case.nc * (case.na - 1)
+    return {"workload": args.workload, "nodes": N, "elements": E, "samples": case.n_samples,
+            "dt": case.dt, "run_steps": case.n_steps, "mass_lumping": case.mass_lumping,
+            "material": "per-element GMRF E and h, seeds %d/%d" % (case.seed_E, case.seed_h),
+            "parallelism": f"replicas{world}",
+            "l2": "per-step state and coefficients > 126 MB L2, no flush"}
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_inputs(case, n_cols):
+    """Mesh and material of the first ``n_cols`` samples of ``case``'s ensemble, made
+    without the product library: the tube geometry (plain NumPy) and the oracle's
+    restatement of the GMRF sampler (the same columns the GPU arm's ensemble has)."""
+    from cvfes_b200.mesh import tube_mesh
+    from oracle.gmrf_oracle import material
+    nodes, elems, inlet, outlet = tube_mesh(case.geometry())
+    E_, h = material(elems, len(nodes), case.n_samples, np.arange(n_cols), case.seed_E,
+                     case.seed_h, case.E0, case.sigma_logE, case.h0, case.sigma_logh, case.tau)
+    coefK = E_ * h
+    gthick = np.repeat(h[:, :, None], 3, axis=2)
+    # row-sum lumping is the reference's own lumping with 3 rho (its assembly applies the
+    # quadrature weight twice, physicsSolver.py:197 and optimizedSolidAssemble.pyx:564-566)
+    rho = case.density * (3.0 if case.mass_lumping == "rowsum" else 1.0)
+    return nodes, elems, np.concatenate([inlet, outlet]), coefK, gthick, rho
+
+
 def cpu_reference_run(case, S_cpu, n_steps, warmup, threads=None):
     """Time the reference's CPU solid step (its compiled MultiplyByVector plus the NumPy
-    update of physicsSolver.py:263-292) on S_cpu samples of the workload's mesh."""
-    from cvfes_b200.cases import build_mesh
+    update of physicsSolver.py:263-292) on S_cpu samples of the workload."""
     from oracle import solid_oracle as so
     if threads:
         os.environ["OMP_NUM_THREADS"] = str(threads)
-    mesh = build_mesh(case, n_samples=S_cpu)
-    coefK, gthick = mesh.element_coefficients()
+    nodes, elems, bdy, coefK, gthick, rho = reference_inputs(case, S_cpu)
     ref = so.load_reference_module()
     kind = "reference" if ref is not None else "port"
-    o = so.OracleSolidSolver(mesh.nodes, mesh.elementNodeIds, mesh.boundary, coefK, gthick,
-                             mesh.density, mesh.v, mesh.damp, case.dt or 5e-7,
+    if case.dt is None:
+        raise SystemExit("the reference arm needs a workload with a fixed dt")
+    o = so.OracleSolidSolver(nodes, elems, bdy, coefK, gthick, rho, case.nu, case.damp, case.dt,
                              backend="reference" if ref is not None else "numpy")
     pres = case.pressures(warmup + n_steps)
     for n in range(warmup):
@@ -143,6 +199,17 @@ def cpu_reference_run(case, S_cpu, n_steps, warmup, threads=None):
     return S_cpu * n_steps / dt, kind, dt
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args)
     if rank != 0:
@@ -152,54 +219,53 @@ def run_reference(args):
     cores = os.cpu_count()
     S_cpu = args.cpu_samples
     value, kind, secs = cpu_reference_run(case, S_cpu, args.steps, args.warmup, cores)
+    sample = (f"samples 0..{S_cpu - 1} of the {case.n_samples}-sample ensemble, {args.steps} "
+              f"steps after {args.warmup} warm-up; samples never interact, so sample-timesteps/s "
+              f"is linear in the sample count")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": args.workload, "nodes": case.nc * case.na, "samples": S_cpu,
-                   "parallelism": "host threads"},
+        "config": workload_config(args, case, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{S_cpu} of {case.n_samples} samples of {args.workload}, "
-                                   f"{args.steps} steps after {args.warmup} warm-up"},
+                         "cpu": cpu_model(), "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_gpu(args):
+# ------------------------------------------------------------------ GPU arm
+class _Clock:
+    """The fluid solver's time as ``RefreshContext`` reads it (``physicSolver.t``)."""
+    t = 0.0
+
+
+def gpu_main(args, case, rank, world, local, dev):
     import torch
     import torch.distributed as dist
-    from cvfes_b200 import _lib
-    from cvfes_b200._lib import call, ptr
-    from cvfes_b200.cases import CASES, build_mesh
+    from cvfes_b200.cases import P_MAX, RAMP_STEPS, build_mesh
+    from cvfes_b200.replicas import max_over_ranks, rank_case
     from cvfes_b200.solver import GPUSolidSolver, LocalComm
 
-    rank, world, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=dev)
-    case = CASES[args.workload]
     prec = 32 if args.precision == "fp32" else 64
-    from cvfes_b200.replicas import max_over_ranks, rank_case
     mesh = build_mesh(rank_case(case, rank))
     S, N, E = mesh.nSmp, mesh.nNodes, mesh.nElements
+    dt = case.dt
 
     class Cfg:
-        dt = case.dt or 5e-7
         nSmp = S
         gpu = type("G", (), dict(precision=prec, use_graph=True, graph_chunk=args.chunk,
-                                 watchdog=True, device=local))()
+                                 watchdog=True, device=local, state=args.state))()
         dt_f = 0.01
         exportBdyStressFilename = None
         useConstantStress = False
-        constant_T = 1.0
-        constant_pressure = 0.0
+        # the workload's schedule p_n = P min(n / 100, 1) as RefreshContext's linear ramp
+        constant_pressure = P_MAX
         pressure_ramp = "linear"
+    Cfg.dt = dt
+    Cfg.constant_T = RAMP_STEPS * dt
 
     solver = GPUSolidSolver(LocalComm(), mesh, Cfg)
     K, W = args.steps, args.warmup
@@ -227,137 +293,89 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
-    clocks.stop()
     ck = clocks.summary(t_wall0, t_wall1)
     ms_max = max_over_ranks(ms, dev)
     chunk = args.chunk
-    launches = K + K // chunk + (1 if K % chunk else 0)
-
-    # finite check of the result
+    used_graph = K >= chunk
+    launches = K + (K // chunk + (1 if K % chunk else 0) if used_graph else 1)
     nrm = solver.Norms(check_finite=False)
     finite = bool(np.all(nrm[:, 3] == 0))
 
-    # e2e through the per-step public API: host pressure in, FP64 norms out, every step
+    # e2e through the per-step public API: RefreshContext + Solve, norms out every step
     K2 = args.e2e_steps
-    p_host = torch.empty(1, dtype=torch.float64, pin_memory=True)
-    p_dev = torch.empty(1, dtype=torch.float64, device=dev)
     n_host = torch.empty((S, 4), dtype=torch.float64, pin_memory=True)
-    n_dev = torch.empty((S, 4), dtype=torch.float64, device=dev)
-    fn_step = "cvfes_solid_step_f64" if prec == 64 else "cvfes_solid_step_f32"
-    fn_norm = "cvfes_solid_norms_f64" if prec == 64 else "cvfes_solid_norms_f32"
-    pv = case.pressures(W + K + K2)
+    fluid = _Clock()
+    n0 = max(W, args.chunk) + K  # schedule position after the warm-up and timed steps
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    s = stream.cuda_stream
     for j in range(K2):
-        p_host[0] = pv[W + K + j]
-        p_dev.copy_(p_host, non_blocking=True)
-        call(fn_step, _lib.C.byref(solver._desc), ptr(solver.plan.coef(prec)),
-             ptr(solver.plan.invm(prec)), ptr(solver.bufs[solver.cur]),
-             ptr(solver.bufs[solver.prev]), ptr(solver.bufs[solver.nxt]), ptr(p_dev), None, 0,
-             0.0, None, float(Cfg.dt), float(mesh.damp), s)
-        solver.prev, solver.cur, solver.nxt = solver.cur, solver.nxt, solver.prev
-        call(fn_norm, N, S, ptr(solver.bufs[solver.cur]), ptr(solver.bufs[solver.prev]),
-             ptr(solver.plan.invm(prec)), ptr(solver.norm_work), ptr(n_dev), 0, s)
-        n_host.copy_(n_dev, non_blocking=True)
-        stream.synchronize()
+        fluid.t = (n0 + j) * dt
+        solver.RefreshContext(fluid)
+        solver.Solve(fluid.t, dt)
+        solver.Norms(out=n_host)
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.stop()
     ms2 = max_over_ranks(e0.elapsed_time(e1), dev)
     if world > 1:
         dist.barrier()
     solver.release_graphs()
 
     b = 4 if prec == 32 else 8
-    bstep = algorithmic_bytes(N, E, S, b, b)
+    bstep = algorithmic_bytes(N, E, S, b, b, solver.state_form)
     peaks, peak_kind = measured_peaks()
     achieved = bstep / (ms / K * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(f"{args.workload}_fp{prec}")
-
-    if rank == 0:
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            v, kind, secs = cpu_reference_run(case, args.cpu_samples, args.cpu_steps, 1,
-                                              os.cpu_count())
-            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-                   "sample": f"{args.cpu_samples} of {S} samples of {args.workload}, "
-                             f"{args.cpu_steps} steps, reference MultiplyByVector + NumPy update"}
-        line = {
-            "metric": METRIC, "value": world * S * K / (ms_max * 1e-3), "unit": UNIT,
-            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if prec == 32 else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "nodes": N, "elements": E, "samples": S,
-                       "dt": Cfg.dt, "parallelism": f"replicas{world}",
-                       "l2": "state 3x%.2f GB > L2, no flush" % (3 * N * S * b / 1e9),
-                       "graph_chunk": chunk, "finite": finite},
-            "e2e": {"value": world * S * K2 / (ms2 * 1e-3), "unit": UNIT,
-                    "h2d_bytes_per_step": 8, "d2h_bytes_per_step": S * 4 * 8},
-            "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": traffic, "peak_source": peak_kind,
-                         "bytes_per_step": bstep},
-            "clocks": ck,
-        }
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
-    return 0
+            traffic = json.load(f).get(f"{args.workload}_fp{prec}_{solver.state_form}")
+    out = {
+        "value": world * S * K / (ms_max * 1e-3), "ms_per_step": ms_max / K,
+        "dtype": "f32" if prec == 32 else "f64",
+        "run": {"state_form": solver.state_form, "graph_chunk": chunk,
+                "graph_replays": used_graph, "finite": finite},
+        "e2e": {"value": world * S * K2 / (ms2 * 1e-3), "unit": UNIT, "steps": K2,
+                "path": "RefreshContext + Solve + Norms(out=pinned) per step",
+                "h2d_bytes_per_step": 8, "d2h_bytes_per_step": S * 4 * 8 + 8},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_step_fan", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": traffic, "peak_source": peak_kind, "bytes_per_step": bstep},
+        "clocks": ck,
+    }
+    del solver
+    torch.cuda.empty_cache()
+    return out
 
 
-def adjoint_bytes(N, E, S, b, bt, log_h):
-    """Bytes one reverse step must move: per sample u_n, u_{n+1} read and u_{n-1}
-    written (backward reconstruction, 9N), chi_{n+1}, chi_{n+2} read and chi_n written
-    (9N), inverse mass (N), coefficient (E), the Gamma accumulator read and written
-    (2E) and, for log h, the G accumulator (2N); shared data as in the forward step."""
-    return S * b * (19 * N + 3 * E + (2 * N if log_h else 0)) + E * (12 + 45 * bt) + 3 * N * bt
-
-
-def run_adjoint(args):
-    """Forward + adjoint gradient evaluations of the mismatch objective; a bench step is
-    one evaluation (T forward steps, then T reverse steps and the gradient)."""
+def measure_adjoint(args, workload, prec, rank, world, local, dev, evals, warm):
+    """Forward + adjoint gradient evaluations of the mismatch objective; one evaluation
+    is T forward steps, then T reverse steps and the gradient."""
     import torch
     from cvfes_b200.adjoint import wall_mismatch
     from cvfes_b200.cases import CASES, adjoint_setup
-
-    rank, world, local = dist_setup(args)
-    case = CASES[args.workload]
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
-    prec = 32 if args.precision == "fp32" else 64
     from cvfes_b200.replicas import max_over_ranks, rank_case
+
+    case = CASES[workload]
     problem, logE, logh, _ = adjoint_setup(rank_case(case, rank), precision=prec, device=dev)
     S, N, E, T = problem.S, problem.N, problem.E, problem.T
     log_h = problem.grad_logh
     logE_d, logh_d = logE.to(dev), logh.to(dev)
     stream = torch.cuda.current_stream(dev)
-    K, W = args.steps, args.warmup
-    for _ in range(W):
+    for _ in range(warm):
         problem.objective(logE_d, logh_d)
         problem.gradient()
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
     clocks = ClockSampler(local).start()
     time.sleep(0.6)
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3 * K)]
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3 * evals)]
     t0 = time.perf_counter()
-    for k in range(K):
+    for k in range(evals):
         evs[3 * k].record(stream)
         problem.objective(logE_d, logh_d)
         evs[3 * k + 1].record(stream)
@@ -366,8 +384,8 @@ def run_adjoint(args):
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
     clocks.stop()
-    fwd = sum(evs[3 * k].elapsed_time(evs[3 * k + 1]) for k in range(K))
-    adj = sum(evs[3 * k + 1].elapsed_time(evs[3 * k + 2]) for k in range(K))
+    fwd = sum(evs[3 * k].elapsed_time(evs[3 * k + 1]) for k in range(evals))
+    adj = sum(evs[3 * k + 1].elapsed_time(evs[3 * k + 2]) for k in range(evals))
     ms_tot, ms_fwd, ms_adj = (max_over_ranks(x, dev) for x in (fwd + adj, fwd, adj))
     finite = bool(torch.isfinite(problem.J).all())
 
@@ -377,7 +395,7 @@ def run_adjoint(args):
     gE_h = torch.empty_like(lE_h).pin_memory()
     gh_h = torch.empty_like(lh_h).pin_memory() if log_h else None
     J_h = torch.empty(S, dtype=torch.float64).pin_memory()
-    K2 = max(1, min(K, 2))
+    K2 = max(1, min(evals, 2))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
@@ -396,125 +414,190 @@ def run_adjoint(args):
     torch.cuda.synchronize(dev)
     ms_e2e = e0.elapsed_time(e1)
     problem.release_graphs()
+    del problem
+    torch.cuda.empty_cache()
 
     b = 4 if prec == 32 else 8
     b_fwd = algorithmic_bytes(N, E, S, b, b)
     b_rev = adjoint_bytes(N, E, S, b, b, log_h)
     peaks, peak_kind = measured_peaks()
-    achieved = b_rev / (ms_adj / K / T * 1e-3) / 1e9
-    nck = (T + problem.ckpt_every - 1) // problem.ckpt_every
-    launches_fwd = T + (T // problem.obs_every) + 2 * T // 48 + 4
-    launches_rev = T + (T // problem.obs_every) + 1
-    if rank == 0:
-        line = {
-            "metric": "sample-timesteps/s (fwd+adjoint)",
-            "value": world * S * T * K / (ms_tot * 1e-3), "unit": UNIT,
-            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_tot / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if prec == 32 else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "nodes": N, "elements": E, "samples": S,
-                       "time_steps": T, "dt": problem.dt, "obs_nodes": problem.n_obs,
-                       "obs_every": problem.obs_every, "ckpt_every": problem.ckpt_every,
-                       "checkpoints": nck, "params": "logE,logh" if log_h else "logE",
-                       "parallelism": f"replicas{world}", "l2": "state > L2, no flush",
-                       "finite": finite, "step": "one gradient evaluation (T forward + T "
-                                                 "reverse time steps)"},
-            "adjoint": {"fwd_ms": ms_fwd / K, "adj_ms": ms_adj / K,
-                        "ratio_fwd_plus_adj_over_fwd": ms_tot / ms_fwd,
-                        "gradients_per_s": world * S * K / (ms_tot * 1e-3),
-                        "fwd_sample_timesteps_per_s": world * S * T * K / (ms_fwd * 1e-3),
-                        "fwd_bytes_per_step": b_fwd, "rev_bytes_per_step": b_rev,
-                        "fwd_hbm_frac": b_fwd / (ms_fwd / K / T * 1e-3) / 1e9 / peaks["hbm_gbs"]},
-            "e2e": {"value": world * S * T * K2 / (ms_e2e * 1e-3), "unit": UNIT,
-                    "h2d_bytes_per_step": 2 * E * S * 8,
-                    "d2h_bytes_per_step": (2 if log_h else 1) * E * S * 8 + S * 8},
-            "gpu_launches": K * (launches_fwd + launches_rev),
-            "roofline": {"bound": "hbm", "kernel": "k_reverse (reverse pass average per step)",
-                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                         "peak_source": peak_kind, "bytes_per_step": b_rev},
-            "clocks": clocks.summary(t0, t1),
-        }
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
-    return 0
+    achieved = b_rev / (ms_adj / evals / T * 1e-3) / 1e9
+    return {
+        "workload": workload, "dtype": "f32" if prec == 32 else "f64", "nodes": N,
+        "elements": E, "samples": S, "time_steps": T, "params": "logE,logh" if log_h else "logE",
+        "evaluations": evals, "warmup": warm, "finite": finite,
+        "value": world * S * T * evals / (ms_tot * 1e-3), "unit": "sample-timesteps/s (fwd+adjoint)",
+        "gradients_per_s": world * S * evals / (ms_tot * 1e-3),
+        "fwd_ms": ms_fwd / evals, "adj_ms": ms_adj / evals,
+        "ratio_fwd_plus_adj_over_fwd": ms_tot / ms_fwd,
+        "e2e": {"value": world * S * T * K2 / (ms_e2e * 1e-3), "unit": UNIT,
+                "path": "wall_mismatch autograd.Function, host logE/logh in, gradients out",
+                "h2d_bytes_per_step": 2 * E * S * 8,
+                "d2h_bytes_per_step": (2 if log_h else 1) * E * S * 8 + S * 8},
+        "roofline": {"bound": "hbm", "kernel": "k_reverse (reverse pass, per step)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
+                     "bytes_per_step": b_rev},
+        # forward: T steps, T / obs_every mismatch launches, checkpoint copies and set-up;
+        # reverse: T steps, T / obs_every forcing launches and the gradient reduction
+        "gpu_launches_per_evaluation": (T + T // problem_obs_every(case) + 2 * T // 48 + 4) +
+                                       (T + T // problem_obs_every(case) + 1),
+        "clocks": clocks.summary(t0, t1),
+    }
 
 
-def run_batched(args):
+def problem_obs_every(case):
+    return int(case.extra.get("obs_every", 10))
+
+
+def measure_batched(args, prec, rank, world, local, dev, steps, warm, meshes_cases=None):
     """64 uneven tubes (own resolution, radius, length, sample count and CFL time step)
-    advanced by one persistent launch per step; metric summed over all tubes."""
+    advanced by one persistent launch per launch group and step."""
     import torch
-    import torch.distributed as dist
     from cvfes_b200.batched import BatchedSolidSolver
-    from cvfes_b200.cases import P_MAX, RAMP_STEPS, batched_cases, build_meshes, case_dt
+    from cvfes_b200.cases import P_MAX, RAMP_STEPS, case_dt
+    from cvfes_b200.replicas import max_over_ranks
     from cvfes_b200.tune import tune_batch
 
-    rank, world, local = dist_setup(args)
-    cases = batched_cases(64, seed=7 + 1000 * rank)
-    meshes = build_meshes(cases)  # spawn pool, before any CUDA work of this process
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
-    prec = 32 if args.precision == "fp32" else 64
+    cases, meshes = meshes_cases
     dts = [case_dt(c, m) for c, m in zip(cases, meshes)]
-    batch = BatchedSolidSolver(meshes, dts, precision=prec, device=dev, graph_chunk=args.chunk)
+    batch = BatchedSolidSolver(meshes, dts, precision=prec, device=dev, graph_chunk=48,
+                               state=args.state)
     tuned = tune_batch(batch)
-    K, W = args.steps, args.warmup
-    pres = P_MAX * np.minimum(np.arange(W + K, dtype=np.float64) / RAMP_STEPS, 1.0)
+    pres = P_MAX * np.minimum(np.arange(warm + steps, dtype=np.float64) / RAMP_STEPS, 1.0)
     stream = torch.cuda.current_stream(dev)
-    batch.Advance(pres[:W])
+    batch.Advance(pres[:warm])
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
     clocks = ClockSampler(local).start()
     time.sleep(0.6)
     t0 = time.perf_counter()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    batch.Advance(pres[W:W + K])
+    batch.Advance(pres[warm:warm + steps])
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
     clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    from cvfes_b200.replicas import max_over_ranks
     ms_max = max_over_ranks(ms, dev)
     finite = all(bool(np.all(n[:, 3] == 0)) for n in batch.Norms(check_finite=False))
     S_total = batch.sample_count()
     bstep = batch.algorithmic_bytes()
     peaks, peak_kind = measured_peaks()
-    achieved = bstep / (ms / K * 1e-3) / 1e9
-    # per launch group: one step kernel per step, one clock kernel per graph chunk and
-    # per plain remainder
+    achieved = bstep / (ms / steps * 1e-3) / 1e9
     n_groups = len(batch.groups)
-    launches = n_groups * (K + K // batch.graph_chunk + 1)
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": world * S_total * K / (ms_max * 1e-3), "unit": UNIT,
-            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if prec == 32 else "f64", "data": "synthetic",
-            "config": {"workload": "batched64", "tubes": len(cases),
-                       "nodes": sum(m.nNodes for m in meshes),
-                       "elements": sum(m.nElements for m in meshes), "samples": S_total,
-                       "parallelism": f"replicas{world}", "kernel": ("fan" if batch.variant == 1
-                                                                    else "row gather"),
-                       "vec": tuned.get("vec"), "grid": tuned.get("grid"),
-                       "launch_groups": n_groups,
-                       "l2": "state > L2, no flush",
-                       "finite": finite},
-            "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                         "peak_source": peak_kind, "bytes_per_step": bstep},
-            "clocks": clocks.summary(t0, t1),
-        }
-        print(json.dumps(line), flush=True)
+    out = {
+        "workload": "batched64", "dtype": "f32" if prec == 32 else "f64",
+        "tubes": len(meshes), "nodes": sum(m.nNodes for m in meshes),
+        "elements": sum(m.nElements for m in meshes), "samples": S_total,
+        "steps": steps, "warmup": warm, "finite": finite, "state_form": batch.state_form,
+        "value": world * S_total * steps / (ms_max * 1e-3), "unit": UNIT,
+        "ms_per_step": ms_max / steps,
+        "kernel": "fan" if batch.variant == 1 else "row gather", "vec": tuned.get("vec"),
+        "grid": tuned.get("grid"), "launch_groups": n_groups,
+        "gpu_launches": n_groups * (steps + steps // batch.graph_chunk + 1),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "peak_source": peak_kind, "bytes_per_step": bstep},
+        "clocks": clocks.summary(t0, t1),
+    }
     batch.release_graphs()
+    del batch
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from cvfes_b200.cases import CASES, batched_cases, build_meshes
+
+    rank, world, local = dist_setup(args)
+    legs = set(args.legs.split(","))
+    meshes_cases = None
+    if "batched" in legs:
+        # the batch's GMRF material in a spawn pool, before any CUDA work of this process
+        cases = batched_cases(64, seed=7 + 1000 * rank)
+        meshes_cases = (cases, build_meshes(cases))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    case = CASES[args.workload]
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic",
+            "config": workload_config(args, case, world)}
+    if "main" in legs:
+        line.update(gpu_main(args, case, rank, world, local, dev))
+    if "adjoint" in legs:
+        line["adjoint"] = {
+            "fp32": measure_adjoint(args, "adjoint64", 32, rank, world, local, dev,
+                                    args.adj_evals, 1),
+            "fp64": measure_adjoint(args, "adjoint64", 64, rank, world, local, dev,
+                                    args.adj_evals, 1)}
+    if "batched" in legs:
+        line["batched"] = measure_batched(args, 32, rank, world, local, dev, args.batch_steps,
+                                          48, meshes_cases)
+    if rank == 0 and world == 1 and "main" in legs and not args.no_cpu_baseline:
+        v, kind, secs = cpu_reference_run(case, args.cpu_samples, args.cpu_steps, 1,
+                                          os.cpu_count())
+        line["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": kind, "cpu": cpu_model(),
+            "sample": f"samples 0..{args.cpu_samples - 1} of the {case.n_samples}-sample "
+                      f"ensemble, {args.cpu_steps} steps after 1 warm-up, reference "
+                      f"MultiplyByVector + NumPy update (linear in the sample count)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_workload(args):
+    """A single non-default workload as its own line (adjoint or batched)."""
+    import torch
+    import torch.distributed as dist
+    from cvfes_b200.cases import CASES, batched_cases, build_meshes
+
+    rank, world, local = dist_setup(args)
+    meshes_cases = None
+    if args.workload == "batched64":
+        cases = batched_cases(64, seed=7 + 1000 * rank)
+        meshes_cases = (cases, build_meshes(cases))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=dev)
+    prec = 32 if args.precision == "fp32" else 64
+    if args.workload == "batched64":
+        r = measure_batched(args, prec, rank, world, local, dev, args.steps, args.warmup,
+                            meshes_cases)
+        metric = METRIC
+        cfg = {"workload": "batched64", "tubes": r["tubes"], "nodes": r["nodes"],
+               "elements": r["elements"], "samples": r["samples"],
+               "parallelism": f"replicas{world}"}
+    else:
+        r = measure_adjoint(args, args.workload, prec, rank, world, local, dev, args.steps,
+                            args.warmup)
+        metric = "sample-timesteps/s (fwd+adjoint)"
+        c = CASES[args.workload]
+        cfg = {"workload": args.workload, "nodes": r["nodes"], "elements": r["elements"],
+               "samples": r["samples"], "time_steps": r["time_steps"], "params": r["params"],
+               "parallelism": f"replicas{world}",
+               "step": "one gradient evaluation (T forward + T reverse time steps)",
+               "obs_every": problem_obs_every(c)}
+    if rank == 0:
+        line = {"metric": metric, "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": r["dtype"], "data": "synthetic",
+                "config": cfg, "result": r, "roofline": r["roofline"], "clocks": r["clocks"]}
+        if "e2e" in r:
+            line["e2e"] = r["e2e"]
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -528,22 +611,25 @@ def main():
     ap.add_argument("--impl", default="cvfes_b200", choices=["cvfes_b200", "reference"])
     ap.add_argument("--workload", default="tube256x1024")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--state", default="auto", choices=["auto", "previous", "velocity"])
     ap.add_argument("--chunk", type=int, default=48)
     ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--legs", default="main,adjoint,batched",
+                    help="legs of the default line: main, adjoint, batched")
+    ap.add_argument("--adj-evals", type=int, default=3)
+    ap.add_argument("--batch-steps", type=int, default=96)
     ap.add_argument("--cpu-samples", type=int, default=4)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
-    if args.chunk % 3:
-        raise SystemExit("--chunk must be a multiple of 3")
+    if args.chunk % 6:
+        raise SystemExit("--chunk must be a multiple of 6")
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "batched64":
-        return run_batched(args)
-    if args.workload in ("adjoint64", "stenosed512x2048"):
-        return run_adjoint(args)
+    if args.workload in ("batched64", "adjoint64", "stenosed512x2048"):
+        return run_workload(args)
     return run_gpu(args)
 
 

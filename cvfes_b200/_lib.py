@@ -55,6 +55,8 @@ class SolidMeshDesc(C.Structure):
         ("tile_we", C.c_int32),
         ("tile_pad", C.c_int32),
         ("bandwidth", C.c_int64),
+        ("state_form", C.c_int32),
+        ("state_pad", C.c_int32),
     ]
 
 
@@ -128,6 +130,8 @@ SIGNATURES = {
     "cvfes_solid_norms_f64": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
     "cvfes_solid_norms_f32": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
     "cvfes_solid_norms_noalloc_f32": (C.c_int, [I64, I64, P, P, P, P, I32, P]),
+    "cvfes_solid_norms_vel_f64": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
+    "cvfes_solid_norms_vel_f32": (C.c_int, [I64, I64, P, P, P, P, P, I32, P]),
     "cvfes_graph_capture_advance": (C.c_int, [DESC, I32, P, P, P, P, P, P, P, I64, D, D, P,
                                               C.POINTER(C.c_void_p)]),
     "cvfes_graph_launch": (C.c_int, [P, P]),
@@ -137,6 +141,7 @@ SIGNATURES = {
     "cvfes_set_step_prefetch": (C.c_int, [I32, I32, I32]),
     "cvfes_get_step_prefetch": (C.c_int, [I32, P, P]),
     "cvfes_status_read": (C.c_int, [P, P]),
+    "cvfes_set_wait_probe": (C.c_int, [I32]),
     "cvfes_batch_table_bytes": (C.c_int64, [I32]),
     "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, P]),
     "cvfes_batch_step": (C.c_int, [P, I32, P, I32, I32, I32, I32, P, I64, I32, P]),

@@ -31,11 +31,11 @@ from .solver import GPUSolidSolver, LocalComm
 
 
 class _Cfg:
-    def __init__(self, dt, nSmp, precision, device):
+    def __init__(self, dt, nSmp, precision, device, state="auto"):
         self.dt = dt
         self.nSmp = nSmp
         self.gpu = type("G", (), dict(precision=precision, use_graph=False, graph_chunk=48,
-                                      watchdog=True, device=device))()
+                                      watchdog=True, device=device, state=state))()
         self.pressure_ramp = "linear"
 
 
@@ -70,17 +70,18 @@ class BatchedSolidSolver:
     def __init__(self, meshes: Sequence, dts: Sequence[float], precision: int = 32,
                  device="cuda:0", vec: Optional[int] = None, grid: int = 0,
                  graph_chunk: int = 48, max_steps: int = 8192, variant: int = 1,
-                 grouped: bool = True):
+                 grouped: bool = True, state: str = "auto"):
         if len(meshes) != len(dts) or not meshes:
             raise ValueError("one dt per mesh")
-        if graph_chunk % 3:
-            raise ValueError("graph_chunk must be a multiple of 3")
+        if graph_chunk % 6:
+            raise ValueError("graph_chunk must be a multiple of 6")
         self.device = torch.device(device)
         self.precision = precision
         idx = self.device.index or 0
         self.solvers: List[GPUSolidSolver] = [
-            GPUSolidSolver(LocalComm(), m, _Cfg(float(dt), m.nSmp, precision, idx))
+            GPUSolidSolver(LocalComm(), m, _Cfg(float(dt), m.nSmp, precision, idx, state))
             for m, dt in zip(meshes, dts)]
+        self.state_form = self.solvers[0].state_form
         self.dts = [float(d) for d in dts]
         maxv = 4 if precision == 32 else 2
         if vec is None:
@@ -179,8 +180,8 @@ class BatchedSolidSolver:
                 g.clock.zero_()
             done = 0
             chunk = self.graph_chunk
-            if use_graph and n >= chunk + 2:
-                lead = (3 - self.rot) % 3  # plain steps until the rotation is back at 0
+            if use_graph and n >= chunk + 5:
+                lead = (6 - self.rot) % 6  # plain steps until the rotation is back at 0
                 if lead:
                     self._plain(lead)
                     done += lead
@@ -192,11 +193,20 @@ class BatchedSolidSolver:
             if n - done:
                 self._plain(n - done)
         self.steps += n
-        cur = (3 - self.rot) % 3
-        for s in self.solvers:
-            s.cur, s.prev, s.nxt = cur, (cur + 1) % 3, (cur + 2) % 3
-            s.step_count = self.steps
+        self.sync_roles()
         return self
+
+    def sync_roles(self):
+        """Set each mesh solver's buffer roles from the batch's rotation phase
+        (``rot`` = steps taken mod 6; the rule of ``cvfes_batch_step``)."""
+        for s in self.solvers:
+            if s.state_form == "velocity":
+                s.cur, s.prev = (2 if self.rot & 1 else 0), 1
+                s.nxt = 2 - s.cur
+            else:
+                cur = (3 - self.rot % 3) % 3
+                s.cur, s.prev, s.nxt = cur, (cur + 1) % 3, (cur + 2) % 3
+            s.step_count = self.steps
 
     def _graph(self, g: _Group, chunk):
         key = (chunk, self.vec, self.grid, self.variant)
@@ -229,12 +239,14 @@ class BatchedSolidSolver:
         return [s.Norms(check_finite) for s in self.solvers]
 
     def algorithmic_bytes(self) -> int:
-        """Bytes one batched step must move (sum of the per-mesh step formula)."""
+        """Bytes one batched step must move (sum of the per-mesh step formula; the
+        velocity-state form reads and writes the increment as well: 13N per sample)."""
         b = 4 if self.precision == 32 else 8
         tot = 0
         for s in self.solvers:
             N, E, S = s.lclNNodes, s.nElms, s.nSmp
-            tot += S * b * (10 * N + E) + E * (12 + 45 * b) + 3 * N * b
+            state = 13 * N if s.state_form == "velocity" else 10 * N
+            tot += S * b * (state + E) + E * (12 + 45 * b) + 3 * N * b
         return tot
 
     def sample_count(self) -> int:

@@ -9,7 +9,8 @@ headers.  Sections offer ConfigObj's ``as_int``/``as_float``/``as_bool`` and
 The config classes keep the reference's attribute names (``cvconfig.py:17-219``)
 and add two optional sections used only by this package:
 
-* ``[gpu]``: ``precision`` (fp64 | fp32), ``use_graph``, ``graph_chunk``,
+* ``[gpu]``: ``precision`` (fp64 | fp32), ``state`` (auto | previous | velocity),
+  ``use_graph``, ``graph_chunk``,
   ``norms_every``, ``watchdog``, ``device``;
 * ``[synthetic]``: a structured tube wall mesh with GMRF material samples in
   place of the VTP files the reference reads (see :mod:`cvfes_b200.cases`).
@@ -242,6 +243,12 @@ class GPUConfig:
         self.norms_every = sec.get_int("norms_every", 0)
         self.watchdog = sec.get_bool("watchdog", True)
         self.device = sec.get_int("device", -1)
+        # second state buffer of the template step: previous (u_{n-1}, the reference's
+        # pair of displacements), velocity (the increment u_n - u_{n-1}, kept in its
+        # own buffer) or auto (velocity for the FP32 state, previous for FP64)
+        self.state = sec.get_str("state", "auto").lower()
+        if self.state not in ("auto", "previous", "velocity"):
+            raise ValueError("[gpu] state must be auto, previous or velocity")
 
 
 class CVConfig:

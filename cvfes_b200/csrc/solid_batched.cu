@@ -9,7 +9,8 @@
 // thread runs the same row gather K_s u_s and fused damped update as the
 // single-mesh L1 kernel, so a mesh advanced in a batch is bitwise identical to the
 // same mesh advanced alone.  All meshes rotate their three state buffers in lock
-// step; the rotation index and the step's offset into the pressure schedules are
+// step (the rotation phase is the step count mod 6, which fixes the roles of both
+// state forms); the phase and the step's offset into the pressure schedules are
 // launch arguments (a device clock supplies the base offset inside CUDA graphs).
 //
 // Two kernels walk the items.  The gather kernel (variant 0) runs the single-mesh L1
@@ -47,7 +48,7 @@ struct BatchMesh {
     int tpn;     // threads per node chunk
     int npb;     // nodes per block
     int chunks;  // sample chunks per node block (the last one may be partial)
-    int pad;
+    int form;    // 1: velocity-state form (buf[1] holds the increment), 0: u_{n-1} in buf
     // fan kernel layout: items of kBatchWarps warps, f_npw nodes per warp
     long long f_off;  // first fan item of this mesh
     int f_tpn;        // lanes per node (min(32, S/VEC))
@@ -58,6 +59,23 @@ struct BatchMesh {
 };
 
 constexpr int kBatchWarps = 2;
+
+// Buffer roles of a mesh at rotation phase rot = (steps taken) % 6.  Previous-
+// displacement form: u_n = buf[(3 - rot % 3) % 3], u_{n-1} the next one, u_{n+1} the
+// one after.  Velocity-state form: the increment stays in buf[1] and u_n alternates
+// between buf[0] (even phases) and buf[2] (odd phases).
+__device__ __forceinline__ void batch_roles(const BatchMesh& M, int rot, int& cur, int& prev,
+                                            int& nxt) {
+    if (M.form) {
+        cur = (rot & 1) ? 2 : 0;
+        prev = 1;
+        nxt = 2 - cur;
+    } else {
+        cur = (3 - rot % 3) % 3;
+        prev = (cur + 1) % 3;
+        nxt = (cur + 2) % 3;
+    }
+}
 
 __device__ __forceinline__ int batch_mesh_of(const BatchMesh* __restrict__ tab, int n_meshes,
                                              long long w, bool fan) {
@@ -74,10 +92,11 @@ template <typename T, int V, bool DIFF>
 __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restrict__ tab,
                                                      int n_meshes, long long total, int rot,
                                                      const long long* clock, long long j) {
-    const int cur = (3 - rot) % 3, prev = (cur + 1) % 3, nxt = (cur + 2) % 3;
     const long long base = clock ? clock[0] : 0LL;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const BatchMesh& M = tab[batch_mesh_of(tab, n_meshes, w, false)];
+        int cur, prev, nxt;
+        batch_roles(M, rot, cur, prev, nxt);
         const long long local = w - M.item_off;
         const long long nb = local / M.chunks;
         const int chunk = (int)(local - nb * M.chunks);
@@ -97,6 +116,7 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restric
         A.u = static_cast<const T*>(M.buf[cur]);
         A.up = static_cast<const T*>(M.buf[prev]);
         A.un = static_cast<T*>(M.buf[nxt]);
+        A.vel = M.form ? static_cast<T*>(M.buf[prev]) : nullptr;
         A.trac = nullptr;
         A.p_sched = M.p_sched;
         A.clock = nullptr;
@@ -112,9 +132,7 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restric
         const size_t col = (size_t)vec * V;
         const size_t row = (size_t)a * 3 * S + col;
         if (a < M.n_clamped) {
-            const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+            clamp_store<T, V>(A, S, row);
             continue;
         }
         Vec<T, V> ua[3];
@@ -160,7 +178,6 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int cur = (3 - rot) % 3, prev = (cur + 1) % 3, nxt = (cur + 2) % 3;
     const long long base = clock ? clock[0] : 0LL;
     const size_t stage_bytes = (size_t)cap * (16 + kSlabStride * sizeof(T));
     // stage q: barrier at smem + 8q, records then stiffness rows at smem + 16 + q * stage_bytes
@@ -181,6 +198,8 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
         if (threadIdx.x == 0 && wn < total)
             batch_fan_issue<T>(tab, n_meshes, wn, cap, bar0 + 8 * (sg ^ 1), stage_rec(srec0, stage_bytes, sg ^ 1), stage_slab(sslab0, stage_bytes, sg ^ 1));
         const BatchMesh& M = tab[batch_mesh_of(tab, n_meshes, w, true)];
+        int cur, prev, nxt;
+        batch_roles(M, rot, cur, prev, nxt);
         const long long local = w - M.f_off;
         const long long nb = local / M.f_chunks;
         const int chunk = (int)(local - nb * M.f_chunks);
@@ -199,6 +218,7 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
         A.u = static_cast<const T*>(M.buf[cur]);
         A.up = static_cast<const T*>(M.buf[prev]);
         A.un = static_cast<T*>(M.buf[nxt]);
+        A.vel = M.form ? static_cast<T*>(M.buf[prev]) : nullptr;
         A.trac = nullptr;
         A.p_sched = M.p_sched;
         A.clock = nullptr;
@@ -231,9 +251,7 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
         }
         if (active) {
             if (clamped) {
-                const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+                clamp_store<T, V>(A, S, row);
             } else {
                 const int kb = __ldg(M.node_ptr + a0);
                 const int k0 = __ldg(M.node_ptr + a) - kb, k1 = __ldg(M.node_ptr + a + 1) - kb;
@@ -381,7 +399,9 @@ extern "C" int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes,
         b.tpn = sv < 32 ? sv : 32;
         b.npb = 256 / b.tpn;
         b.chunks = (sv + b.tpn - 1) / b.tpn;
-        b.pad = 0;
+        if (ms.state_form != 0 && ms.state_form != 1)
+            return fail(CVFES_ERR_ARG, "cvfes_batch_pack: mesh %d state_form", m);
+        b.form = ms.state_form;
         b.item_off = off;
         off += ((ms.n_nodes + b.npb - 1) / b.npb) * b.chunks;
         b.f_tpn = sv < 32 ? sv : 32;
@@ -407,7 +427,7 @@ extern "C" int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes,
 extern "C" int cvfes_batch_step(const void* table_dev, int32_t n_meshes, const int64_t* totals,
                                 int32_t precision, int32_t vec, int32_t variant, int32_t rot,
                                 const int64_t* clock, int64_t j, int32_t grid, void* stream) {
-    if (!table_dev || n_meshes <= 0 || !totals || rot < 0 || rot > 2 ||
+    if (!table_dev || n_meshes <= 0 || !totals || rot < 0 || rot > 5 ||
         (precision != 32 && precision != 64) || (vec != 1 && vec != 2 && vec != 4) ||
         (precision == 64 && vec == 4) || (variant != 0 && variant != 1))
         return fail(CVFES_ERR_ARG, "cvfes_batch_step: bad argument");
@@ -434,14 +454,14 @@ extern "C" int cvfes_batch_advance(const void* table_dev, int32_t n_meshes,
                                    const int64_t* totals, int32_t precision, int32_t vec,
                                    int32_t variant, int32_t rot0, int64_t* clock, int64_t n_steps,
                                    int32_t grid, int32_t* rot_out, void* stream) {
-    if (n_steps < 0 || rot0 < 0 || rot0 > 2)
+    if (n_steps < 0 || rot0 < 0 || rot0 > 5)
         return fail(CVFES_ERR_ARG, "cvfes_batch_advance: bad argument");
     int rot = rot0;
     for (long long k = 0; k < n_steps; ++k) {
         int rc = cvfes_batch_step(table_dev, n_meshes, totals, precision, vec, variant, rot,
                                   clock, k, grid, stream);
         if (rc) return rc;
-        rot = (rot + 1) % 3;
+        rot = (rot + 1) % 6;
     }
     if (clock && n_steps > 0) {
         k_batch_clock_add<<<1, 1, 0, (cudaStream_t)stream>>>(reinterpret_cast<long long*>(clock),
@@ -456,9 +476,9 @@ extern "C" int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes
                                          const int64_t* totals, int32_t precision, int32_t vec,
                                          int32_t variant, int64_t* clock, int64_t chunk,
                                          int32_t grid, cvfes_graph** out) {
-    if (!out || chunk <= 0 || chunk % 3 || !clock)
+    if (!out || chunk <= 0 || chunk % 6 || !clock)
         return fail(CVFES_ERR_ARG,
-                    "cvfes_batch_graph_capture: chunk must be a positive multiple of 3 and a "
+                    "cvfes_batch_graph_capture: chunk must be a positive multiple of 6 and a "
                     "clock is required");
     cudaStream_t cs;
     CVFES_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

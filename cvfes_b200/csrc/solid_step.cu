@@ -42,9 +42,7 @@ __global__ void __launch_bounds__(256) k_step(StepArgs<T> A) {
     const size_t col = (size_t)vec * V;
     const size_t row = (size_t)a * 3 * S + col;
     if (a < A.n_clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        clamp_store<T, V>(A, S, row);
         return;
     }
     Vec<T, V> ua[3];
@@ -150,9 +148,10 @@ __global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
     const uint32_t bar = smem_u32(smem);
     int4* srec = reinterpret_cast<int4*>(smem + 16);
     T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
-    if (threadIdx.x == 0) mbar_init(bar, 1);
+    const bool probe = A.probe_polls > 0;
+    if (threadIdx.x == 0) mbar_init(bar, probe ? 2 : 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !probe) {
         const uint32_t b_rec = (uint32_t)nsl * 16u;
         const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
         mbar_arrive_expect_tx(bar, b_rec + b_slab);
@@ -184,9 +183,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_staged(StepArgs<T> A) {
     }
     if (!active) return;
     if (clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        clamp_store<T, V>(A, S, row);
         return;
     }
     Vec<T, V> acc[3];
@@ -221,10 +218,11 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// u_prev = u0 - dt du0 + dt^2/2 ddu0, ddu0 = (p0 f - damp m du0 - K u0)/m  (0 where m == 0).
+// u_prev = u0 - dt du0 + dt^2/2 ddu0, ddu0 = (p0 f - damp m du0 - K u0)/m  (0 where m == 0);
+// in the velocity-state form (vel) the increment u0 - u_prev = dt du0 - dt^2/2 ddu0 instead.
 template <typename T>
 __global__ void k_init(const T* fhat, const T* invm, const T* u0, const T* du0, const T* ku,
-                       T* u_prev, long long n_nodes, int S, T p0, T dt, T damp) {
+                       T* u_prev, long long n_nodes, int S, T p0, T dt, T damp, int vel) {
     const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long a = g / S;
     if (a >= n_nodes) return;
@@ -236,7 +234,8 @@ __global__ void k_init(const T* fhat, const T* invm, const T* u0, const T* du0, 
         const T m = im != T(0) ? T(1) / im : T(0);
         const T rhs = p0 * fhat[4 * a + d] - damp * m * du0[o] - ku[o];
         const T acc = im != T(0) ? rhs * im : T(0);
-        u_prev[o] = u0[o] - dt * du0[o] + T(0.5) * dt * dt * acc;
+        u_prev[o] = vel ? dt * du0[o] - T(0.5) * dt * dt * acc
+                        : u0[o] - dt * du0[o] + T(0.5) * dt * dt * acc;
     }
 }
 
@@ -288,9 +287,10 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     const uint32_t bar = smem_u32(smem);
     int4* srec = reinterpret_cast<int4*>(smem + 16);
     T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
-    if (threadIdx.x == 0) mbar_init(bar, 1);
+    const bool probe = A.probe_polls > 0;
+    if (threadIdx.x == 0) mbar_init(bar, probe ? 2 : 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !probe) {
         const uint32_t b_rec = (uint32_t)nsl * 16u;
         const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
         mbar_arrive_expect_tx(bar, b_rec + b_slab);
@@ -318,15 +318,13 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     }
     if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
         fan_prefetch(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
-    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+    if (!mbar_wait_bounded(bar, 0, probe ? A.probe_polls : kMaxPolls)) {
         if (lane == 0 && A.status) atomicOr(A.status, 1);
         return;
     }
     if (!active) return;
     if (clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        clamp_store<T, V>(A, S, row);
         return;
     }
     Vec<T, V> acc[3];
@@ -412,9 +410,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
         }
         if (active) {
             if (clamped) {
-                const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+                clamp_store<T, V>(A, S, row);
             } else {
                 const int kb = __ldg(A.node_ptr + a0);
                 const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
@@ -455,9 +451,10 @@ __global__ void __launch_bounds__(256, MINB) k_step_burst(StepArgs<T> A) {
     const uint32_t bar = smem_u32(smem);
     int4* srec = reinterpret_cast<int4*>(smem + 16);
     T* sslab = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
-    if (threadIdx.x == 0) mbar_init(bar, 1);
+    const bool probe = A.probe_polls > 0;
+    if (threadIdx.x == 0) mbar_init(bar, probe ? 2 : 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !probe) {
         const uint32_t b_rec = (uint32_t)nsl * 16u;
         const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
         mbar_arrive_expect_tx(bar, b_rec + b_slab);
@@ -489,9 +486,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_burst(StepArgs<T> A) {
     }
     if (!active) return;
     if (clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        clamp_store<T, V>(A, S, row);
         return;
     }
     const int k0 = __ldg(A.node_ptr + a) - kb;
@@ -690,9 +685,7 @@ __global__ void __launch_bounds__(256, 1) k_step_pipe(PipeArgs<T> P) {
         const size_t col = ((size_t)chunk * 32 + lane) * V;
         const size_t row = (size_t)a * 3 * S + col;
         if (a < A.n_clamped) {
-            const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+            clamp_store<T, V>(A, S, row);
         } else {
             const unsigned char* ln = sb + lane * V * sizeof(T);
             const int4* srec = reinterpret_cast<const int4*>(sb + P.rec_off);
@@ -822,9 +815,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_gather(StepArgs<T> A) {
     }
     if (!active) return;
     if (clamped) {
-        const Vec<T, V> cl = vfill<T, V>(A.clamp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stcs<T, V>(A.un + row + d * S, cl);
+        clamp_store<T, V>(A, S, row);
         return;
     }
     // issue the whole gather
@@ -932,7 +923,8 @@ inline long long norm_chunks(long long n_nodes) {
     return std::max(1LL, std::min(1024LL, c));
 }
 
-template <typename T>
+// VEL: `up` holds the increment v = u_n - u_{n-1} (velocity-state form), else u_{n-1}.
+template <typename T, bool VEL>
 __global__ void k_norms_partial(long long n_nodes, int S, long long npc, const T* __restrict__ u,
                                 const T* __restrict__ up, const T* __restrict__ invm,
                                 double* __restrict__ work) {
@@ -951,7 +943,8 @@ __global__ void k_norms_partial(long long n_nodes, int S, long long npc, const T
             const double x = (double)u[o], y = (double)up[o];
             if (!isfinite(x)) nf += 1.0;
             su += x * x;
-            dv2 += (x - y) * (x - y);
+            const double dv = VEL ? y : x - y;
+            dv2 += dv * dv;
         }
         sv += dv2;
         sm += m * dv2;
@@ -1018,6 +1011,8 @@ static StepTuning g_tune64 = {2, 2, 3, 2};
 // node rows alone speed the reverse step up by 2.4%.
 static int g_pf_dist[2] = {-1, -1};
 static int g_pf_parts[2] = {-1, -1};
+// Polls of the failure-path test of the fan kernel's bounded wait (0: off).
+static int g_wait_probe = 0;
 Prefetch step_prefetch(int precision, long long bandwidth) {
     const int q = precision == 32 ? 0 : 1;
     Prefetch p{g_pf_dist[q], g_pf_parts[q]};
@@ -1211,11 +1206,31 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     A.w0 = (T)(dt * dt / (1.0 + g));
     A.status = m->status;
     A.cap_slots = 0;
+    if (m->state_form != 0 && m->state_form != 1)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_step: state_form must be 0 or 1");
+    if (m->state_form == 1) {
+        if (up == u || up == un)
+            return fail(CVFES_ERR_ARG, "cvfes_solid_step: the increment buffer must be its own");
+        A.vel = const_cast<T*>(up);
+    }
     const void* ptrs[6] = {coef, invm, u, up, un, nullptr};
     StepTuning tune = tuning_of<T>();
+    // The velocity-state form is fused into the kernels that share step_epilogue; the
+    // cp.async-gather (2), pipelined (4) and TMA-tiled (7) variants run the fan kernel.
+    if (A.vel && (tune.staged == 2 || tune.staged == 4 || tune.staged == 7)) {
+        tune.staged = 3;
+        tune.minb = 2;
+    }
     const Prefetch pf = step_prefetch(sizeof(T) == 4 ? 32 : 64, m->bandwidth);
     A.pf_dist = pf.dist;
     A.pf_parts = pf.parts;
+    A.probe_polls = g_wait_probe;
+    if (A.probe_polls > 0) {  // only the fan kernel has the probe; it needs a status word
+        if (!A.status)
+            return fail(CVFES_ERR_ARG, "cvfes_solid_step: the wait probe needs a status word");
+        tune.staged = 3;
+        tune.minb = 2;
+    }
     int V = pick_vec<T>(ptrs, 5, A.S);
     while (V > tune.vec) V /= 2;
     constexpr bool DIFF = std::is_same<T, float>::value;
@@ -1280,6 +1295,10 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
         }
         return rc;
     }
+    if (A.probe_polls > 0)
+        return fail(CVFES_ERR_UNSUPPORTED,
+                    "cvfes_solid_step: the wait probe needs the fan kernel (S / vec a multiple "
+                    "of 32 and the mesh's max_degree)");
     V = V_rows;
     const int block = 256;
     const RowGrid rg = row_grid(m->n_nodes, A.S / V, block);
@@ -1334,10 +1353,17 @@ int launch_advance(const cvfes_solid_mesh* m, const T* coef, const T* invm, T* b
     if (!p_sched) return fail(CVFES_ERR_ARG, "cvfes_solid_advance: needs a pressure schedule");
     T* buf[3] = {b0, b1, b2};
     int cur = 0, prev = 1, nxt = 2;
+    const bool vel = m && m->state_form == 1;
     for (long long j = 0; j < n_steps; ++j) {
         int rc = launch_step<T>(m, coef, invm, buf[cur], buf[prev], buf[nxt], p_sched, clock, j,
                                 0.0, nullptr, dt, damp, st);
         if (rc) return rc;
+        if (vel) {  // the increment stays in place; the displacement buffers swap
+            const int t = cur;
+            cur = nxt;
+            nxt = t;
+            continue;
+        }
         const int old_prev = prev;
         prev = cur;
         cur = nxt;
@@ -1364,14 +1390,14 @@ int launch_init(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     const int block = 256;
     k_init<T><<<grid_1d(m->n_nodes * S, block), block, 0, st>>>(
         static_cast<const T*>(m->fhat), invm, u0, du0, work, u_prev, m->n_nodes, S, (T)p0, (T)dt,
-        (T)damp);
+        (T)damp, m->state_form == 1 ? 1 : 0);
     CVFES_LAUNCH_CHECK("k_init");
     return CVFES_OK;
 }
 
 template <typename T>
 int launch_norms(long long n_nodes, long long S, const T* u, const T* up, const T* invm,
-                 double* work, double* out, int check_finite, cudaStream_t st) {
+                 double* work, double* out, int check_finite, cudaStream_t st, bool vel = false) {
     if (n_nodes <= 0 || S <= 0 || S > INT32_MAX || !u || !up || !invm || !work || !out)
         return fail(CVFES_ERR_ARG, "cvfes_solid_norms: bad argument");
     const long long nch = norm_chunks(n_nodes);
@@ -1379,7 +1405,12 @@ int launch_norms(long long n_nodes, long long S, const T* u, const T* up, const 
     double* total = work + (size_t)nch * S * 4;
     CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
     dim3 grid((unsigned)nch, (unsigned)((S + kNormThreads - 1) / kNormThreads));
-    k_norms_partial<T><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, up, invm, work);
+    if (vel)
+        k_norms_partial<T, true><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, up, invm,
+                                                                work);
+    else
+        k_norms_partial<T, false><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, up, invm,
+                                                                 work);
     CVFES_LAUNCH_CHECK("k_norms_partial");
     k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
     CVFES_LAUNCH_CHECK("k_norms_final");
@@ -1491,6 +1522,18 @@ extern "C" int cvfes_solid_norms_f32(int64_t n_nodes, int64_t n_samples, const f
     return launch_norms<float>(n_nodes, n_samples, u, u_prev, invm, work, out, check_finite,
                                (cudaStream_t)stream);
 }
+extern "C" int cvfes_solid_norms_vel_f64(int64_t n_nodes, int64_t n_samples, const double* u,
+                                         const double* vel, const double* invm, double* work,
+                                         double* out, int32_t check_finite, void* stream) {
+    return launch_norms<double>(n_nodes, n_samples, u, vel, invm, work, out, check_finite,
+                                (cudaStream_t)stream, true);
+}
+extern "C" int cvfes_solid_norms_vel_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                                         const float* vel, const float* invm, double* work,
+                                         double* out, int32_t check_finite, void* stream) {
+    return launch_norms<float>(n_nodes, n_samples, u, vel, invm, work, out, check_finite,
+                               (cudaStream_t)stream, true);
+}
 
 // ------------------------------------------------------------------ CUDA graphs
 
@@ -1500,10 +1543,14 @@ extern "C" int cvfes_graph_capture_advance(const cvfes_solid_mesh* mesh, int32_t
                                            int64_t* clock, int64_t chunk, double dt, double damp,
                                            void* stream, cvfes_graph** out) {
     (void)stream;
-    if (!out || chunk <= 0 || chunk % 3 != 0 || !clock)
+    // the buffers must be back in their places after a chunk: a period of 3 steps in the
+    // previous-displacement form, 2 in the velocity-state form
+    const int period = (mesh && mesh->state_form == 1) ? 2 : 3;
+    if (!out || chunk <= 0 || chunk % period != 0 || !clock)
         return fail(CVFES_ERR_ARG,
-                    "cvfes_graph_capture_advance: chunk must be a positive multiple of 3 and a "
-                    "clock is required");
+                    "cvfes_graph_capture_advance: chunk must be a positive multiple of %d and a "
+                    "clock is required",
+                    period);
     if (precision != 32 && precision != 64)
         return fail(CVFES_ERR_ARG, "cvfes_graph_capture_advance: precision must be 32 or 64");
     cudaStream_t cs;
@@ -1616,6 +1663,13 @@ extern "C" int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int
     return CVFES_OK;
 }
 
+extern "C" int cvfes_set_wait_probe(int32_t polls) {
+    if (polls < 0 || polls > (1 << 20))
+        return fail(CVFES_ERR_ARG, "cvfes_set_wait_probe: polls must be 0..2^20");
+    g_wait_probe = polls;
+    return CVFES_OK;
+}
+
 extern "C" int cvfes_status_read(int32_t* status, void* stream) {
     if (!status) return fail(CVFES_ERR_ARG, "cvfes_status_read: null status");
     int32_t h = 0;
@@ -1689,8 +1743,8 @@ extern "C" int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples,
     double* total = work + (size_t)nch * S * 4;  // the non-finite counter starts at zero
     CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
     dim3 grid((unsigned)nch, (unsigned)((S + kNormThreads - 1) / kNormThreads));
-    k_norms_partial<float><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, u_prev, invm,
-                                                          work);
+    k_norms_partial<float, false><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, u_prev,
+                                                                 invm, work);
     CVFES_LAUNCH_CHECK("k_norms_partial (fixed scratch)");
     k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
     CVFES_LAUNCH_CHECK("k_norms_final (fixed scratch)");

@@ -43,6 +43,18 @@ struct StepArgs {
     int pf_dist = 0;  // fan kernel: nodes ahead whose rows are prefetched into L2 (0: off)
     int pf_parts = 0; // bit 0: node rows; bit 1: element coefficient rows
     int pf_group = 1; // node blocks covered by one prefetching block
+    // Velocity-state form (null: the second state buffer `up` holds u_{n-1}).  When set
+    // it equals `up`, which then holds the increment v_n = u_n - u_{n-1}: the step reads
+    // it and writes v_{n+1} back in place (each row is read and written by its owner
+    // thread only), and u_{n+1} = u_n + v_{n+1} goes to `un`.  The increment is then
+    // never rebuilt from two rounded displacements, so the FP32 rounding of u does not
+    // feed back into the velocity.
+    T* vel = nullptr;
+    // Failure-path test of the bounded waits (0: off).  When > 0 the fan kernel sets
+    // its stage barrier up for two arrivals, issues no copy and waits at most this many
+    // polls: the wait gives up with nothing in flight, the kernel records bit 0 in
+    // `status` and returns without writing the step.
+    int probe_polls = 0;
 };
 
 // ------------------------------------------------------------ TMA / mbarrier helpers
@@ -297,12 +309,44 @@ __device__ __forceinline__ void step_update(const StepArgs<T>& A, size_t S, size
     }
 }
 
-// As step_update, reading the row's u_{n-1} and inverse mass here.
+// Dirichlet row: u_{n+1} = clamp; in the velocity-state form also v_{n+1} = clamp - u_n.
+template <typename T, int V>
+__device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size_t row) {
+    const Vec<T, V> cl = vfill<T, V>(A.clamp);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (A.vel) stcs<T, V>(A.vel + row + d * S, vsub(cl, ldg<T, V>(A.u + row + d * S)));
+        stcs<T, V>(A.un + row + d * S, cl);
+    }
+}
+
+// As step_update, reading the row's u_{n-1} (or v_n) and inverse mass here.
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
                                               const Vec<T, V> (&acc)[3], const T (&f)[3]) {
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
+    if (A.vel) {
+        // velocity-state form: v_{n+1} = v_n (1 - eta) + w (p f - K u_n), u_{n+1} = u_n + v_{n+1};
+        // a row without mass (u_{n+1} = 0) keeps v_{n+1} = -u_n, the exact increment.
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const Vec<T, V> vo = ldcs<T, V>(A.up + row + d * S);
+            const T load = f[d];
+            Vec<T, V> o, vn;
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                const T w = A.w0 * im.v[i];
+                const T v = fma(w, load - acc[d].v[i], fma(-A.eta, vo.v[i], vo.v[i]));
+                const bool live = im.v[i] != T(0);
+                o.v[i] = live ? ua[d].v[i] + v : T(0);
+                vn.v[i] = live ? v : -ua[d].v[i];
+            }
+            stcs<T, V>(A.un + row + d * S, o);
+            stcs<T, V>(A.vel + row + d * S, vn);
+        }
+        return;
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const Vec<T, V> up = ldcs<T, V>(A.up + row + d * S);

@@ -19,7 +19,10 @@ Differences by design:
   assembled once on the undeformed wall (stiffness update interval 0, the
   default), or, with ``stiffness_update_interval`` n >= 1, rebuilt matrix-free with
   the follower pressure on ``x + u`` every n steps (n = 1: ``assemble_K_P``);
-* FP64 (default) or FP32 state, chosen by ``[gpu] precision``.
+* FP64 (default) or FP32 state, chosen by ``[gpu] precision``;
+* the second state buffer holds u_{n-1} as in the reference, or (``[gpu] state``
+  velocity, the default for the FP32 state) the increment v_n = u_n - u_{n-1},
+  updated in place, so the FP32 rounding of u is not fed back into the velocity.
 """
 from __future__ import annotations
 
@@ -104,6 +107,11 @@ class GPUSolidSolver(PhysicsSolver):
         self.use_graph = getattr(gpu, "use_graph", True)
         self.graph_chunk = getattr(gpu, "graph_chunk", 48)
         self.watchdog = getattr(gpu, "watchdog", True)
+        # stiffness_update_interval (cvconfig.py:154): 0 keeps the undeformed stiffness and
+        # load (linear templates); n >= 1 rebuilds both on x + u every n steps
+        self.update_interval = int(getattr(config, "update_interval", 0) or 0)
+        self.state_form = resolve_state_form(getattr(gpu, "state", "auto"), self.precision,
+                                             self.update_interval)
         self.InitializeSync()
         if self.InitializeGPU(getattr(gpu, "device", -1)) < 0:
             raise RuntimeError("GPUSolidSolver: no usable CUDA device")
@@ -114,9 +122,6 @@ class GPUSolidSolver(PhysicsSolver):
         self.constant_T = getattr(config, "constant_T", 1.0)
         self.constantPressure = getattr(config, "constant_pressure", 0.0)
         self.pressure_ramp = getattr(config, "pressure_ramp", "cosine")
-        # stiffness_update_interval (cvconfig.py:154): 0 keeps the undeformed stiffness and
-        # load (linear templates); n >= 1 rebuilds both on x + u every n steps
-        self.update_interval = int(getattr(config, "update_interval", 0) or 0)
         self.nt = 0
         if self.stressFilename is not None:
             if self.useConstantStress:
@@ -178,7 +183,7 @@ class GPUSolidSolver(PhysicsSolver):
                                   mass_lumping=getattr(m, "mass_lumping", "reference"))
             coefK, gthick = m.element_coefficients()
             self.plan.set_material(coefK, gthick)
-            self._desc = self.plan.desc(self.precision)
+            self.refresh_desc()
             dtype = torch.float64 if self.precision == 64 else torch.float32
             S, ndof = self.nSmp, self.lclNDof
             self.bufs = [torch.zeros((ndof, S), dtype=dtype, device=dev) for _ in range(3)]
@@ -200,6 +205,7 @@ class GPUSolidSolver(PhysicsSolver):
                 device=dev)
             self._graphs = {}
             self._p_buf = None
+            self._norm_out = None
             self.step_count = 0
             self.geo_counter = 0
             self.geo_live = False
@@ -216,6 +222,13 @@ class GPUSolidSolver(PhysicsSolver):
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
+
+    def refresh_desc(self):
+        """Rebuild the C mesh descriptor from the plan (after the plan's tiling or set-up
+        arrays change), with this solver's state form."""
+        self._desc = self.plan.desc(self.precision)
+        self._desc.state_form = 1 if self.state_form == "velocity" else 0
+        return self._desc
 
     # ------------------------------------------------------------------ per step
     def RefreshContext(self, physicSolver):
@@ -284,14 +297,28 @@ class GPUSolidSolver(PhysicsSolver):
                  ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), None, None, 0,
                  float(self.pressure), ptr(self.trac_dev), float(dt), float(self.damp),
                  self._stream())
-        self.prev, self.cur, self.nxt = self.cur, self.nxt, self.prev
+        self._rotate()
         self.step_count += 1
+
+    def _rotate(self):
+        """Buffer roles after one template step: (u_n, u_{n-1}, free) <- (u_{n+1}, u_n,
+        u_{n-1}); in the velocity-state form the increment stays where it is and the two
+        displacement buffers swap."""
+        if self.state_form == "velocity":
+            self.cur, self.nxt = self.nxt, self.cur
+        else:
+            self.prev, self.cur, self.nxt = self.cur, self.nxt, self.prev
 
     def Advance(self, pressures, dt: Optional[float] = None, use_graph: Optional[bool] = None):
         """Many steps with a per-step pressure schedule, no host work between steps.
 
         With ``use_graph`` the steps run as replays of one captured CUDA graph of
-        ``graph_chunk`` steps (a multiple of 3); the remainder runs as plain launches.
+        ``graph_chunk`` steps (a multiple of 3; in the velocity-state form the least
+        common multiple of it and 2); the remainder runs as plain launches.
+
+        With a nodal traction set (``RefreshContext`` of a traction series), the
+        traction is held for the whole call: the steps run as single launches with the
+        schedule's pressures, and ``RefreshContext`` is not re-run between them.
         """
         dt = self.dt if dt is None else dt
         use_graph = self.use_graph if use_graph is None else use_graph
@@ -300,8 +327,9 @@ class GPUSolidSolver(PhysicsSolver):
         prec = self.precision
         if self.update_interval > 0:
             if self.trac_dev is not None:  # per-step launches with the held traction
+                ph = p.cpu().numpy()
                 for j in range(n):
-                    self.pressure = float(pressures[j])
+                    self.pressure = float(ph[j])
                     self.Solve(None, dt)
                 return self
             return self._advance_geo(p, n, dt)
@@ -309,6 +337,8 @@ class GPUSolidSolver(PhysicsSolver):
             self.clock.zero_()
             done = 0
             chunk = self.graph_chunk
+            if self.state_form == "velocity" and chunk % 2:
+                chunk *= 2
             if use_graph and self.trac_dev is None and n >= chunk:
                 key = (chunk, float(dt), self.cur, self.prev, self.nxt, p.data_ptr())
                 g = self._graphs.get(key)
@@ -327,12 +357,14 @@ class GPUSolidSolver(PhysicsSolver):
                 while n - done >= chunk:
                     call("cvfes_graph_launch", g, self._stream())
                     done += chunk
+            self.step_count += done
             if n - done > 0:
                 cur_idx = _lib.C.c_int32()
                 prev_idx = _lib.C.c_int32()
-                if self.trac_dev is not None:
+                if self.trac_dev is not None:  # Solve counts its own steps
+                    ph = p.cpu().numpy()
                     for j in range(done, n):
-                        self.pressure = float(pressures[j])
+                        self.pressure = float(ph[j])
                         self.Solve(None, dt)
                 else:
                     fn = "cvfes_solid_advance_f64" if prec == 64 else "cvfes_solid_advance_f32"
@@ -345,7 +377,7 @@ class GPUSolidSolver(PhysicsSolver):
                          self._stream())
                     self.cur, self.prev = order[cur_idx.value], order[prev_idx.value]
                     self.nxt = 3 - self.cur - self.prev
-            self.step_count += n
+                    self.step_count += n - done
         return self
 
     def _advance_geo(self, p, n, dt):
@@ -398,17 +430,31 @@ class GPUSolidSolver(PhysicsSolver):
             pass
 
     # ------------------------------------------------------------------ outputs
-    def Norms(self, check_finite: Optional[bool] = None) -> np.ndarray:
-        """FP64 per-sample (sum u^2, sum du^2, sum m du^2, #non-finite), shape (S, 4)."""
-        out = torch.empty((self.nSmp, 4), dtype=torch.float64, device=self.device)
+    def Norms(self, check_finite: Optional[bool] = None,
+              out: Optional[torch.Tensor] = None) -> np.ndarray:
+        """FP64 per-sample (sum u^2, sum du^2, sum m du^2, #non-finite), shape (S, 4).
+
+        ``out``: an (S, 4) FP64 host tensor (pinned, for an asynchronous copy) that
+        receives the result; the call returns once it has arrived."""
+        if self._norm_out is None:
+            self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
+                                         device=self.device)
+        dev_out = self._norm_out
         fn = "cvfes_solid_norms_f64" if self.precision == 64 else "cvfes_solid_norms_f32"
+        if self.state_form == "velocity":
+            fn = fn.replace("norms_", "norms_vel_")
         chk = self.watchdog if check_finite is None else check_finite
         with torch.cuda.device(self.device):
             call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
                  ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
-                 ptr(self.norm_work), ptr(out), int(bool(chk)), self._stream())
+                 ptr(self.norm_work), ptr(dev_out), int(bool(chk)), self._stream())
+            if out is None:
+                res = dev_out.cpu()
+            else:
+                out.copy_(dev_out, non_blocking=True)
+                res = out
             self.plan.check_status()
-        return out.cpu().numpy()
+        return res.numpy()
 
     def LambdaMax(self, iters: int = 200, seed: int = 0) -> np.ndarray:
         """Largest eigenvalue of M⁻¹K per sample on the free dofs (FP64 power iteration
@@ -492,6 +538,21 @@ class GPUSolidSolver(PhysicsSolver):
                               resU.T.reshape(self.nSmp, self.mesh.nNodes, self.Dof),
                               stress=stress)
         self.comm.Barrier()
+
+
+def resolve_state_form(state: str, precision: int, update_interval: int) -> str:
+    """``[gpu] state``: ``auto`` is the velocity-state form for the FP32 state of the
+    template step and the previous-displacement form otherwise (FP64 state, or the
+    geometric mode, whose kernels keep the reference's pair of displacements)."""
+    state = (state or "auto").lower()
+    if state not in ("auto", "previous", "velocity"):
+        raise ValueError("state must be auto, previous or velocity")
+    if state == "velocity" and update_interval > 0:
+        raise ValueError("the velocity-state form is for the template step "
+                         "(stiffness_update_interval 0)")
+    if state == "auto":
+        return "velocity" if precision == 32 and update_interval == 0 else "previous"
+    return state
 
 
 def C_desc(desc):

@@ -73,7 +73,8 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
     """Pick (variant, vec, npb, minb) for ``solver``'s precision and problem shape."""
     prec = solver.precision
     dev = solver.device
-    shape = ("step", prec, solver.lclNNodes, solver.nElms, solver.nSmp, solver.plan.max_degree)
+    shape = ("step", prec, solver.lclNNodes, solver.nElms, solver.nSmp, solver.plan.max_degree,
+             solver.state_form)
     key = _key("step", dev, shape)
     cache = _load_cache() if use_cache else {}
     if key in cache:
@@ -132,7 +133,8 @@ def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
                use_cache: bool = True, variants: Optional[Sequence[int]] = None) -> dict:
     """Pick the batch's kernel, samples per thread and persistent grid size."""
     dev = batch.device
-    shape = ("batch", batch.precision, tuple((s.lclNNodes, s.nElms, s.nSmp) for s in batch.solvers))
+    shape = ("batch", batch.precision, batch.state_form,
+             tuple((s.lclNNodes, s.nElms, s.nSmp) for s in batch.solvers))
     key = _key("batch", dev, shape)
     cache = _load_cache() if use_cache else {}
     if key in cache:
@@ -149,7 +151,7 @@ def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
                  1: list(grids) if grids is not None else [0, 4 * sms]}
     saved = [[b.clone() for b in s.bufs] for s in batch.solvers]
     rot0 = batch.rot
-    pres = np.zeros(steps + batch.graph_chunk + 2)
+    pres = np.zeros(steps + batch.graph_chunk + 6)
     results = []
     for variant, vec, grid in [(v, x, g) for v in variants for x in vecs for g in grid_sets[v]]:
         batch.set_launch(vec=vec, grid=grid, variant=variant)
@@ -157,7 +159,7 @@ def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
             for b, x in zip(s.bufs, sv):
                 b.copy_(x)
         batch.rot = rot0
-        batch.Advance(pres[:batch.graph_chunk + 2])
+        batch.Advance(pres[:batch.graph_chunk + 6])
         ms = _time_ms(lambda: batch.Advance(pres[:steps]), dev) / steps
         results.append((ms, dict(variant=variant, vec=vec, grid=grid, ms_per_step=ms)))
     for s, sv in zip(batch.solvers, saved):
@@ -166,9 +168,10 @@ def tune_batch(batch, vecs: Optional[Sequence[int]] = None,
     batch.rot = rot0
     best = min(results, key=lambda r: r[0])[1]
     batch.set_launch(vec=best["vec"], grid=best["grid"], variant=best["variant"])
-    cur = (3 - batch.rot) % 3
+    steps0 = batch.steps
+    batch.sync_roles()
     for s in batch.solvers:
-        s.cur, s.prev, s.nxt = cur, (cur + 1) % 3, (cur + 2) % 3
+        s.step_count = steps0
     if use_cache:
         _store(key, best)
     return dict(best, cached=False, tried=[r[1] for r in results])

@@ -72,6 +72,11 @@ typedef struct cvfes_solid_mesh {
     int64_t        bandwidth;     /* max |a - b| over the element edges between
                                      unclamped nodes (0: unknown; sets the automatic
                                      L2 prefetch distance of the fan step kernels) */
+    int32_t        state_form;    /* what the second state buffer of the template step
+                                     holds: 0 = u_{n-1} (the reference's pair of
+                                     displacements), 1 = the increment v_n = u_n - u_{n-1},
+                                     updated in place by each step (velocity-state form) */
+    int32_t        state_pad;
 } cvfes_solid_mesh;
 
 /* Step-kernel tuning (the autotuner sets these; defaults: variant 3, FP32 vec 4,
@@ -122,6 +127,15 @@ int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t
  * made after the call (graphs keep what they captured).                        */
 int cvfes_set_step_prefetch(int32_t precision, int32_t distance, int32_t parts);
 int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int32_t* parts);
+
+/* Failure-path test of the bounded device waits; no counterpart in the reference.
+ * With polls > 0, template steps made after the call run the fan kernel with its
+ * shared-memory stage barrier set up for two arrivals and no copy issued, waiting at
+ * most `polls` polls: every block's wait gives up with nothing in flight, sets bit 0
+ * of the mesh's status word (which must be non-NULL) and returns without writing
+ * u_next.  cvfes_status_read then reports CVFES_ERR_TIMEOUT.  0 (the default) turns
+ * it off.  Applies to launches made after the call (graphs keep what they captured). */
+int cvfes_set_wait_probe(int32_t polls);
 
 /* Read and clear the device status word of a mesh descriptor (synchronises the
  * stream).  Returns CVFES_ERR_TIMEOUT if a bounded device wait gave up since
@@ -243,7 +257,12 @@ int cvfes_solid_kmul_f32(const cvfes_solid_mesh* mesh, const float* coef,
  * Pressure is p_sched[clock[0] + j] (device f64 schedule, device int64 clock)
  * or, when p_sched is NULL, the value `pressure`.  trac (device T [N][4] or
  * NULL) adds an external nodal traction dt^2 * trac / (m (1+dt/2 damp))
- * (calc_u_appTrac, physicsSolverSDampGPUs.cl:436-446).                        */
+ * (calc_u_appTrac, physicsSolverSDampGPUs.cl:436-446).
+ * With mesh->state_form == 1 (velocity-state form) `u_prev` holds the increment
+ * v_n = u_n - u_{n-1} instead and is overwritten in place with v_{n+1}
+ * (u_next = u + v_{n+1}); it must not alias u or u_next.  The same update, with
+ * the increment carried in its own buffer rather than rebuilt from two rounded
+ * displacements.                                                                */
 int cvfes_solid_step_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
                          const double* u, const double* u_prev, double* u_next,
                          const double* p_sched, const int64_t* clock, int64_t j,
@@ -259,7 +278,9 @@ int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef, const 
  * of physicsSolverSDampGPUs.py:398-399.  bufs[0] = u_n, bufs[1] = u_{n-1},
  * bufs[2] = free on entry; on return *rot tells which: u_n is bufs[(rot+0)%3]...
  * precisely, after k steps u_n is bufs[(3 - k % 3) % 3] — returned as *cur_idx,
- * u_{n-1} as *prev_idx.  After the steps the clock (if given) advances by n_steps. */
+ * u_{n-1} as *prev_idx.  In the velocity-state form bufs[1] holds the increment for
+ * good and u_n alternates between bufs[0] and bufs[2] (*prev_idx stays 1).  After the
+ * steps the clock (if given) advances by n_steps.                                  */
 int cvfes_solid_advance_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
                             double* buf0, double* buf1, double* buf2,
                             const double* p_sched, int64_t* clock, int64_t n_steps,
@@ -273,7 +294,8 @@ int cvfes_solid_advance_f32(const cvfes_solid_mesh* mesh, const float* coef, con
 
 /* Initial state u_{-1} = u0 - dt du0 + dt^2/2 ddu0 with ddu0 = (p0 fhat - damp m du0 - K u0)/m
  * (LocalInitialize, physicsSolver.py:209-230; calc_ddu, physicsSolverSDampGPUs.cl:398-409).
- * u0, du0 device T [3N][S]; writes u_prev.  Uses `work` T [3N][S] for K u0.  */
+ * u0, du0 device T [3N][S]; writes u_prev (in the velocity-state form the increment
+ * u0 - u_{-1} = dt du0 - dt^2/2 ddu0).  Uses `work` T [3N][S] for K u0.         */
 int cvfes_solid_init_f64(const cvfes_solid_mesh* mesh, const double* coef, const double* invm,
                          const double* u0, const double* du0, double* u_prev, double* work,
                          double p0, double dt, double damp, void* stream);
@@ -295,6 +317,14 @@ int cvfes_solid_norms_f64(int64_t n_nodes, int64_t n_samples, const double* u,
 int cvfes_solid_norms_f32(int64_t n_nodes, int64_t n_samples, const float* u,
                           const float* u_prev, const float* invm, double* work,
                           double* out, int32_t check_finite, void* stream);
+/* The same norms for the velocity-state form: `vel` holds the increment v = u_n - u_{n-1},
+ * so out[s][1] = sum v^2 and out[s][2] = sum m v^2.                             */
+int cvfes_solid_norms_vel_f64(int64_t n_nodes, int64_t n_samples, const double* u,
+                              const double* vel, const double* invm, double* work,
+                              double* out, int32_t check_finite, void* stream);
+int cvfes_solid_norms_vel_f32(int64_t n_nodes, int64_t n_samples, const float* u,
+                              const float* vel, const float* invm, double* work,
+                              double* out, int32_t check_finite, void* stream);
 
 /* The FP32-state norms of cvfes_solid_norms_f32 without a workspace argument and
  * without allocating anything; no counterpart in the reference.  For callers that
@@ -312,7 +342,8 @@ int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples, const floa
 
 /* ------------------------------------------------------------ CUDA graphs
  * Capture `chunk` steps of cvfes_solid_advance (chunk a multiple of 3 so the
- * buffer roles repeat) plus the clock increment into one executable graph.
+ * buffer roles repeat; of 2 in the velocity-state form) plus the clock increment
+ * into one executable graph.
  * Each cvfes_graph_launch advances `chunk` steps.  precision: 32 or 64.       */
 typedef struct cvfes_graph cvfes_graph;
 int cvfes_graph_capture_advance(const cvfes_solid_mesh* mesh, int32_t precision,
@@ -333,8 +364,9 @@ int cvfes_graph_destroy(cvfes_graph* g);
  * items of the fan kernel (variant 1: blocks of 2 warps, slot rows staged by TMA
  * into two shared-memory stages, fan-rotation gathers), [2] the fan kernel's stage
  * capacity in slots (-1 when a mesh has no max_degree).  All meshes rotate their
- * buffers in lock step: with rot = (steps taken) % 3, u_n = buf[(3-rot)%3],
- * u_{n-1} = buf[(4-rot)%3].  vec: samples per thread (FP32 1|2|4, FP64 1|2), must
+ * buffers in lock step: with rot = (steps taken) % 6, u_n = buf[(3-rot%3)%3],
+ * u_{n-1} = buf[(4-rot%3)%3]; a mesh whose descriptor has state_form 1 keeps its
+ * increment in buf[1] and u_n in buf[0] (rot even) or buf[2] (rot odd).  vec: samples per thread (FP32 1|2|4, FP64 1|2), must
  * divide every mesh's S.  grid: blocks of the persistent launch (<= 0: one block per
  * work item for variant 0, as many as fit for variant 1).  Both variants give the
  * same bits as the single-mesh kernels.                                          */
@@ -358,7 +390,7 @@ int cvfes_batch_advance(const void* table_dev, int32_t n_meshes, const int64_t* 
                         int32_t precision, int32_t vec, int32_t variant, int32_t rot0,
                         int64_t* clock, int64_t n_steps, int32_t grid, int32_t* rot_out,
                         void* stream);
-/* `chunk` batched steps (multiple of 3) and the clock increment as one graph. */
+/* `chunk` batched steps (multiple of 6) and the clock increment as one graph. */
 int cvfes_batch_graph_capture(const void* table_dev, int32_t n_meshes, const int64_t* totals,
                               int32_t precision, int32_t vec, int32_t variant, int64_t* clock,
                               int64_t chunk, int32_t grid, cvfes_graph** out);

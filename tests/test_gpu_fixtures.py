@@ -1,0 +1,104 @@
+"""The large workloads over their whole run against the reference's own kernels.
+
+``tests/golden/full_*.npz`` hold, for a seeded chunk of each workload's sample
+ensemble, the state the reference's CPU solid path (its compiled assembly and
+``MultiplyByVector`` with the update of ``physicsSolver.py:263-292``) reached at the
+end of the workload's run: the 256 x 1024 tube after 2000 steps, the stenosed
+512 x 2048 tube after 1000 steps and four tubes of the uneven 64-tube ensemble after
+1000 steps (``tests/golden/make_full_fixtures.py``).
+
+Here the GPU advances the WHOLE ensemble of each workload with the default kernels
+(FP64 state, and the default FP32 state form) and the chunk's samples are compared:
+relative L2 over the fixture's 2048 nodes, and the per-sample sums over all nodes of
+u^2 (and, for FP64, of the last increment squared).  FP64 <= 1e-12, FP32 <= 1e-5.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from cvfes_b200.cases import CASES, batched_cases, build_mesh, case_dt
+from cvfes_b200.solver import GPUSolidSolver, LocalComm
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+FIXTURES = sorted(os.path.basename(p)[5:-4] for p in glob.glob(os.path.join(GOLD, "full_*.npz")))
+TOL = {64: 1e-12, 32: 1e-5}
+
+
+class Cfg:
+    def __init__(self, dt, S, precision):
+        self.dt = dt
+        self.nSmp = S
+        self.gpu = type("G", (), dict(precision=precision, use_graph=True, graph_chunk=48,
+                                      watchdog=True, device=0))()
+        self.pressure_ramp = "linear"
+
+
+def case_of(name):
+    if name.startswith("batch"):
+        return batched_cases(64, seed=7)[int(name[5:])]
+    return CASES[name]
+
+
+_MESHES = {}
+
+
+def workload(name):
+    if name not in _MESHES:
+        _MESHES.clear()  # one workload's material at a time
+        case = case_of(name)
+        mesh = build_mesh(case)
+        _MESHES[name] = (case, mesh, case_dt(case, mesh))
+    return _MESHES[name]
+
+
+def material_checksum(coefK, gthick):
+    E = coefK.shape[0]
+    picks = [0, E // 2, E - 1]
+    out = []
+    for a in (coefK, gthick):
+        a = np.asarray(a, dtype=np.float64).reshape(E, a.shape[1], -1)[:, :, 0]
+        out.append(np.stack([a.sum(axis=0), (a * a).sum(axis=0), *[a[i] for i in picks]]))
+    return np.concatenate(out)
+
+
+def test_fixtures_present():
+    assert len(FIXTURES) >= 3, FIXTURES
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("name", FIXTURES)
+def test_full_run_against_reference(lib, cuda, name, precision):
+    fx = dict(np.load(os.path.join(GOLD, f"full_{name}.npz")))
+    case, mesh, dt = workload(name)
+    idx = fx["samples"]
+    assert mesh.nSmp == int(fx["n_samples"])
+    assert abs(dt - float(fx["dt"])) <= 1e-14 * dt
+    coefK, gthick = mesh.element_coefficients()
+    chk = material_checksum(coefK[:, idx], gthick[:, idx])
+    assert np.allclose(chk, fx["material"], rtol=1e-12, atol=0), "material differs"
+    s = GPUSolidSolver(LocalComm(), mesh, Cfg(dt, mesh.nSmp, precision))
+    s.Advance(case.pressures(int(fx["n_steps"])))
+    nrm = s.Norms()
+    inv = np.empty(s.lclNDof, dtype=np.int64)
+    inv[s.dofs] = np.arange(s.lclNDof)
+    dofs = (3 * fx["nodes"][:, None] + np.arange(3)[None, :]).ravel()
+    rows = torch.from_numpy(inv[dofs]).to(cuda)
+    cols = torch.from_numpy(idx.astype(np.int64)).to(cuda)
+    u = s.local_displacement()[rows][:, cols].double().cpu().numpy()
+    s.release_graphs()
+    ref = fx["u_subset"]
+    err = float(np.linalg.norm(u - ref) / np.linalg.norm(ref))
+    e_u2 = float(np.max(np.abs(nrm[idx, 0] - fx["sum_u2"]) / fx["sum_u2"]))
+    e_du2 = float(np.max(np.abs(nrm[idx, 1] - fx["sum_du2"]) / fx["sum_du2"]))
+    print(f"\n{name} FP{precision} ({s.state_form}), samples {idx.tolist()}, "
+          f"{int(fx['n_steps'])} steps: rel-L2 {err:.3e}, sum u^2 {e_u2:.3e}, "
+          f"sum du^2 {e_du2:.3e}")
+    assert np.all(nrm[:, 3] == 0)
+    assert err <= TOL[precision]
+    assert e_u2 <= 2 * TOL[precision]
+    if precision == 64:
+        assert e_du2 <= 2 * TOL[precision]

@@ -500,7 +500,7 @@ def test_tiled_step_with_outliers_matches_fan(lib, cuda, precision):
         s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
         s.plan.build_tiles(P=16, H=18, W=1, EH=36, WE=1)
         assert s.plan.tile_stats["node_outliers"] > 0 and s.plan.tile_stats["element_outliers"] > 0
-        s._desc = s.plan.desc(precision)
+        s.refresh_desc()
         s.Advance(pres)
         s.plan.check_status()
     finally:

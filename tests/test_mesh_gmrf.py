@@ -129,3 +129,20 @@ def test_solid_mesh_nodal_coefficients():
                   vthickness=np.full((N, S), 2.0))
     coefK, gthick = m.element_coefficients()
     assert np.allclose(coefK, 6.0) and np.allclose(gthick, 2.0)
+
+
+def test_gmrf_matches_oracle_restatement(lib):
+    """The product sampler (selected inversion and Lᵀ solve in the library) against the
+    oracle's C restatement on the same SuperLU factor: marginal variances and samples."""
+    from cvfes_b200.gmrf import ElementGMRF
+    from oracle.gmrf_oracle import GMRFOracle, load_library
+    if load_library() is None:
+        pytest.skip("oracle/_ref/libgmrf_oracle.so not built (make -C oracle restatement)")
+    nodes, elems, _, _ = tube_mesh(TubeGeometry(24, 20, 3.0))
+    g = ElementGMRF(elems, len(nodes))
+    o = GMRFOracle(elems, len(nodes))
+    v, vo = g.variance(), o.marginal_variance()
+    assert np.max(np.abs(v - vo) / vo) < 1e-12
+    z = g.sample(12, seed=5)
+    zo = o.sample(12, seed=5, columns=[0, 7, 11])
+    assert np.max(np.abs(z[:, [0, 7, 11]] - zo)) < 1e-10
