@@ -19,7 +19,10 @@ Metric: sample-timesteps/s = samples x steps / seconds, whole job.
   ``TransientSolverGPU`` drives it: ``RefreshContext(fluid)`` (the pressure of time
   t, passed to the step kernel as a launch argument, 8 bytes) then ``Solve(t, dt)``,
   then ``Norms(out=pinned)`` -- the FP64 per-sample norms and the non-finite
-  watchdog read back into pinned host memory, which synchronises every step.
+  watchdog read back into pinned host memory, which synchronises every step.  The
+  solver runs with ``norms_every = 1``: the persistent fan kernel accumulates the norms
+  while it writes the new state, so they cost no second pass over the state
+  (``--separate-norms``: the separate pass instead).
 * ``adjoint`` (default line): forward + adjoint gradient evaluations of the
   64 x 128 tube, 64 samples, 500 steps (FP32 and FP64): gradients/s, the ratio
   (fwd + adj) / fwd and the reverse pass's bandwidth.
@@ -256,8 +259,11 @@ def gpu_main(args, case, rank, world, local, dev):
 
     class Cfg:
         nSmp = S
+        # norms_every 1: each Solve also produces the FP64 norms of its new state in the
+        # same kernel pass (the e2e leg reads them back every step)
         gpu = type("G", (), dict(precision=prec, use_graph=True, graph_chunk=args.chunk,
-                                 watchdog=True, device=local, state=args.state))()
+                                 watchdog=True, device=local, state=args.state,
+                                 norms_every=0 if args.separate_norms else 1))()
         dt_f = 0.01
         exportBdyStressFilename = None
         useConstantStress = False
@@ -340,7 +346,9 @@ def gpu_main(args, case, rank, world, local, dev):
         "run": {"state_form": solver.state_form, "graph_chunk": chunk,
                 "graph_replays": used_graph, "finite": finite},
         "e2e": {"value": world * S * K2 / (ms2 * 1e-3), "unit": UNIT, "steps": K2,
-                "path": "RefreshContext + Solve + Norms(out=pinned) per step",
+                "path": "RefreshContext + Solve + Norms(out=pinned) per step" +
+                        (" (norms by a separate pass)" if args.separate_norms else
+                         " (norms fused into the step kernel)"),
                 "h2d_bytes_per_step": 8, "d2h_bytes_per_step": S * 4 * 8 + 8},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_step_fan", "achieved": achieved,
@@ -621,6 +629,8 @@ def main():
     ap.add_argument("--cpu-samples", type=int, default=4)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--separate-norms", action="store_true",
+                    help="e2e: norms by a separate pass instead of fused into the step")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

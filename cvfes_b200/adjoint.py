@@ -257,8 +257,12 @@ class _WallMismatch(torch.autograd.Function):
             raise RuntimeError("build the MismatchProblem with grad_logh=True for dJ/dlogh")
         gE, gh = problem.gradient()
         w = gJ.to(torch.float64).reshape(1, -1)
-        return (gE * w if ctx.needs_input_grad[0] else None,
-                gh * w if (gh is not None and ctx.needs_input_grad[1]) else None, None)
+        # gradients in the inputs' own shape and dtype (set_material accepts any shape
+        # that reshapes to (E, S), and autograd wants each gradient like its input)
+        outE = (gE * w).reshape(logE.shape).to(logE.dtype) if ctx.needs_input_grad[0] else None
+        outh = ((gh * w).reshape(logh.shape).to(logh.dtype)
+                if (gh is not None and ctx.needs_input_grad[1]) else None)
+        return outE, outh, None
 
 
 def wall_mismatch(logE: torch.Tensor, logh: torch.Tensor, problem: MismatchProblem) -> torch.Tensor:

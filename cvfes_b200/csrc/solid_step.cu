@@ -25,7 +25,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -269,7 +268,8 @@ __global__ void k_clock_add(long long* clock, long long n) { clock[0] += n; }
 // sample chunk fastest, so the chunks of one node block share its slot rows in L2.
 // With pf_dist > 0 the last warp of the first chunk of every pf_group-th node block
 // prefetches the rows of the pf_group node blocks pf_dist nodes ahead.
-template <typename T, int V, bool DIFF, int MINB>
+// AHEAD = 2: each element's rows are requested two elements ahead (ku_row_fan2).
+template <typename T, int V, bool DIFF, int MINB, int AHEAD = 1>
 __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
@@ -311,9 +311,11 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             ua[d] = ldg<T, V>(A.u + row + d * S);
-            prefetch_l2(A.up + row + d * S);
+            if (A.pf_parts & 4) prefetch_l1(A.up + row + d * S);
+            else prefetch_l2(A.up + row + d * S);
         }
-        prefetch_l2(A.invm + (size_t)a * S + col);
+        if (A.pf_parts & 4) prefetch_l1(A.invm + (size_t)a * S + col);
+        else prefetch_l2(A.invm + (size_t)a * S + col);
         node_load<T>(A, a, step_pressure<T>(A), f);
     }
     if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
@@ -329,7 +331,10 @@ __global__ void __launch_bounds__(256, MINB) k_step_fan(StepArgs<T> A) {
     }
     Vec<T, V> acc[3];
     const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
-    ku_row_fan<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
+    if constexpr (AHEAD == 2)
+        ku_row_fan2<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
+    else
+        ku_row_fan<T, V, DIFF>(srec, sslab, k0, k1, A.u, A.coef, S, col, ua, acc);
     step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
 }
 
@@ -360,6 +365,8 @@ __device__ __forceinline__ void fanp_issue(const StepArgs<T>& A, long long w, ui
     bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
 }
 
+// With A.norm_part (fused norms) the grid is a multiple of nch, so block b always has
+// sample chunk b % nch; its per-lane FP64 sums follow the two stages in shared memory.
 template <typename T, int V, bool DIFF, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long long n_items) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -370,6 +377,13 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
     const uint32_t bar0 = smem_u32(smem);
     int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
     T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    constexpr int kAcc = 4 * V * 32;  // doubles of one warp's norm accumulators
+    double* const nbase = reinterpret_cast<double*>(smem + 16 + 2 * stage_bytes);
+    double* const nacc = A.norm_part ? nbase + warp * kAcc + lane : nullptr;
+    if (nacc) {
+#pragma unroll
+        for (int q = 0; q < 4 * V; ++q) nacc[q * 32] = 0.0;
+    }
     if (threadIdx.x == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
@@ -410,7 +424,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
         }
         if (active) {
             if (clamped) {
-                clamp_store<T, V>(A, S, row);
+                clamp_store<T, V>(A, S, row, nacc, a, col);
             } else {
                 const int kb = __ldg(A.node_ptr + a0);
                 const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
@@ -418,10 +432,21 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
                 ku_row_fan<T, V, DIFF>(stage_rec(srec0, stage_bytes, sg),
                                        stage_slab(sslab0, stage_bytes, sg), k0, k1, A.u, A.coef,
                                        S, col, ua, acc);
-                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f);
+                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f, nacc);
             }
         }
         __syncthreads();
+    }
+    if (A.norm_part) {  // this block's sums over its nodes, warps added in order
+        const int chunk = (int)(blockIdx.x % A.nch);
+        const long long prow = blockIdx.x / A.nch;
+        for (int t = threadIdx.x; t < kAcc; t += blockDim.x) {
+            const int q = t / (32 * V), c = t - q * 32 * V;  // c: sample of the chunk
+            const int ln = c / V, i = c - ln * V;
+            double sum = 0.0;
+            for (int w = 0; w < A.npb; ++w) sum += nbase[w * kAcc + (q * V + i) * 32 + ln];
+            A.norm_part[((size_t)prow * S + (size_t)chunk * 32 * V + c) * 4 + q] = sum;
+        }
     }
 }
 
@@ -1092,9 +1117,12 @@ int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, 
     }
 }
 
+// The persistent fan kernel on as many blocks as are resident (at most one per work
+// item).  With fused norms the grid is rounded down to a multiple of the sample chunks
+// and capped at max_rows chunks' worth, and *rows gets the partial rows written.
 template <typename K, typename T>
 int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStream_t st,
-                  const StepArgs<T>& A) {
+                  const StepArgs<T>& A, long long max_rows, long long* rows) {
     if (smem > 48 * 1024) {
         cudaError_t e =
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1108,6 +1136,12 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
         return fail(CVFES_ERR_CUDA, "k_step_fanp: no resident block fits");
     long long blocks = (long long)per_sm * sm_count();
     if (blocks > n_items) blocks = n_items;
+    if (A.norm_part) {
+        if (blocks > max_rows * A.nch) blocks = max_rows * A.nch;
+        blocks -= blocks % A.nch;
+        if (blocks < A.nch) blocks = A.nch;
+        if (rows) *rows = blocks / A.nch;
+    }
     kernel<<<(unsigned)blocks, threads, smem, st>>>(A, n_items);
     CVFES_LAUNCH_CHECK("k_step_fanp");
     return CVFES_OK;
@@ -1115,12 +1149,21 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
 
 template <typename T, int V, bool DIFF>
 int launch_fanp(int minb, long long n_items, int threads, size_t smem, cudaStream_t st,
-                const StepArgs<T>& A) {
+                const StepArgs<T>& A, long long max_rows = 0, long long* rows = nullptr) {
+    if (A.norm_part) smem += (size_t)A.npb * 4 * V * 32 * sizeof(double);
     switch (minb) {
-        case 4: return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A);
-        case 3: return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A);
-        case 2: return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A);
-        default: return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A);
+        case 4:
+            return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A,
+                                 max_rows, rows);
+        case 3:
+            return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A,
+                                 max_rows, rows);
+        case 2:
+            return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A,
+                                 max_rows, rows);
+        default:
+            return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A,
+                                 max_rows, rows);
     }
 }
 
@@ -1148,6 +1191,14 @@ int launch_staged_v(int variant, int minb, dim3 grid, int threads, size_t smem, 
         if (max_degree <= 6) return launch_burst<T, V, DIFF, 6>(minb, g1, threads, smem, st, A);
         return launch_burst<T, V, DIFF, 8>(minb, g1, threads, smem, st, A);
     }
+    if (variant == 8) {
+        const dim3 g1((unsigned)((long long)grid.x * grid.y));
+        switch (minb) {
+            case 3: return launch_staged(k_step_fan<T, V, DIFF, 3, 2>, g1, threads, smem, st, A);
+            case 2: return launch_staged(k_step_fan<T, V, DIFF, 2, 2>, g1, threads, smem, st, A);
+            default: return launch_staged(k_step_fan<T, V, DIFF, 1, 2>, g1, threads, smem, st, A);
+        }
+    }
     if (variant == 3 || variant == 5) {
         const dim3 g1((unsigned)((long long)grid.x * grid.y));
         switch (minb) {
@@ -1173,10 +1224,16 @@ int launch_staged_v(int variant, int minb, dim3 grid, int threads, size_t smem, 
     }
 }
 
+// norm_work (optional): fuse the per-sample norms of the new state into the step (the
+// persistent fan kernel); *norm_rows gets the partial rows written to norm_work, or 0
+// when the shape has no fused kernel (the caller then runs the separate norms pass).
 template <typename T>
 int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u,
                 const T* up, T* un, const double* p_sched, const long long* clock, long long j,
-                double pressure, const T* trac, double dt, double damp, cudaStream_t st) {
+                double pressure, const T* trac, double dt, double damp, cudaStream_t st,
+                double* norm_work = nullptr, long long* norm_rows = nullptr,
+                long long max_rows = 0) {
+    if (norm_rows) *norm_rows = 0;
     int rc = check_mesh(m, "cvfes_solid_step");
     if (rc) return rc;
     if (!coef || !invm || !u || !up || !un)
@@ -1282,6 +1339,22 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
         A.pf_parts = prefetch_parts(A.pf_parts, A.nch);
         const dim3 grid((unsigned)((m->n_nodes + A.npb - 1) / A.npb), (unsigned)(A.S / V / 32));
         const int threads = 32 * A.npb;
+        if (norm_work && max_rows > 0 && !A.probe_polls) {  // fused norms: persistent fan
+            A.norm_part = norm_work;
+            const long long n_items = (long long)grid.x * grid.y;
+            const size_t smem2 = 16 + 2 * (smem - 16);
+            const int minb = tune.staged == 6 ? tune.minb : 2;
+            if (V == 4) {
+                if constexpr (sizeof(T) == 4)
+                    return launch_fanp<T, 4, DIFF>(minb, n_items, threads, smem2, st, A, max_rows,
+                                                   norm_rows);
+            } else if (V == 2) {
+                return launch_fanp<T, 2, DIFF>(minb, n_items, threads, smem2, st, A, max_rows,
+                                               norm_rows);
+            }
+            return launch_fanp<T, 1, DIFF>(minb, n_items, threads, smem2, st, A, max_rows,
+                                           norm_rows);
+        }
         if (V == 4) {
             if constexpr (sizeof(T) == 4)
                 rc = launch_staged_v<T, 4, DIFF>(tune.staged, tune.minb, grid, threads, smem, st,
@@ -1458,6 +1531,61 @@ extern "C" int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* c
                               damp, (cudaStream_t)stream);
 }
 
+// One step and the FP64 norms of the new state: fused into the persistent fan kernel
+// where the shape allows, else the step followed by the separate norms pass.
+template <typename T>
+int launch_step_norms(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u,
+                      const T* up, T* un, const double* p_sched, const long long* clock,
+                      long long j, double pressure, const T* trac, double dt, double damp,
+                      double* work, double* out, int check_finite, cudaStream_t st) {
+    int rc = check_mesh(m, "cvfes_solid_step_norms");
+    if (rc) return rc;
+    if (!work || !out) return fail(CVFES_ERR_ARG, "cvfes_solid_step_norms: null work or out");
+    const long long N = m->n_nodes, S = m->n_samples;
+    const long long max_rows = norm_chunks(N);  // the rows cvfes_norms_work_size provides
+    long long rows = 0;
+    rc = launch_step<T>(m, coef, invm, u, up, un, p_sched, clock, j, pressure, trac, dt, damp, st,
+                        work, &rows, max_rows);
+    if (rc) return rc;
+    const bool vel = m->state_form == 1;
+    if (rows == 0)  // no fused kernel for this shape: the separate pass over the new state
+        return launch_norms<T>(N, S, un, vel ? up : u, invm, work, out, check_finite, st, vel);
+    double* total = work + (size_t)rows * S * 4;
+    CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
+    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(rows, (int)S, work, out, total);
+    CVFES_LAUNCH_CHECK("k_norms_final");
+    if (check_finite) {
+        double h = 0.0;
+        CVFES_CUDA_TRY(cudaMemcpyAsync(&h, total, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CVFES_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h != 0.0)
+            return fail(CVFES_ERR_NONFINITE, "watchdog: %.0f non-finite state values", h);
+    }
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_solid_step_norms_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                                          const double* invm, const double* u,
+                                          const double* u_prev, double* u_next,
+                                          const double* p_sched, const int64_t* clock, int64_t j,
+                                          double pressure, const double* trac, double dt,
+                                          double damp, double* work, double* out,
+                                          int32_t check_finite, void* stream) {
+    return launch_step_norms<double>(mesh, coef, invm, u, u_prev, u_next, p_sched,
+                                     reinterpret_cast<const long long*>(clock), j, pressure, trac,
+                                     dt, damp, work, out, check_finite, (cudaStream_t)stream);
+}
+extern "C" int cvfes_solid_step_norms_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                                          const float* invm, const float* u, const float* u_prev,
+                                          float* u_next, const double* p_sched,
+                                          const int64_t* clock, int64_t j, double pressure,
+                                          const float* trac, double dt, double damp, double* work,
+                                          double* out, int32_t check_finite, void* stream) {
+    return launch_step_norms<float>(mesh, coef, invm, u, u_prev, u_next, p_sched,
+                                    reinterpret_cast<const long long*>(clock), j, pressure, trac,
+                                    dt, damp, work, out, check_finite, (cudaStream_t)stream);
+}
+
 extern "C" int cvfes_solid_advance_f64(const cvfes_solid_mesh* mesh, const double* coef,
                                        const double* invm, double* buf0, double* buf1,
                                        double* buf2, const double* p_sched, int64_t* clock,
@@ -1619,8 +1747,10 @@ extern "C" int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: npb must be in 1..8");
     if (minb < 1 || minb > 4)
         return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: minb must be in 1..4");
-    if (staged < 0 || staged > 7)
-        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..7");
+    if (staged < 0 || staged > 8)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged must be in 0..8");
+    if (staged == 8 && minb > 3)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_tuning: staged 8 takes minb 1..3");
     StepTuning& t = precision == 32 ? g_tune32 : g_tune64;
     t.vec = vec;
     t.npb = npb;
@@ -1646,8 +1776,8 @@ extern "C" int cvfes_set_step_prefetch(int32_t precision, int32_t distance, int3
         return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: precision must be 32 or 64");
     if (distance < -1 || distance > (1 << 20))
         return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: distance must be in -1..2^20");
-    if (parts < -1 || parts > 3)
-        return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: parts must be in -1..3");
+    if (parts < -1 || parts > 7)
+        return fail(CVFES_ERR_ARG, "cvfes_set_step_prefetch: parts must be in -1..7");
     const int q = precision == 32 ? 0 : 1;
     g_pf_dist[q] = distance;
     g_pf_parts[q] = parts;
@@ -1693,30 +1823,22 @@ extern "C" int cvfes_status_read(int32_t* status, void* stream) {
 constexpr long long kNormScratchDoubles = 1LL << 19;
 static __device__ __align__(256) double g_norm_scratch[kNormScratchDoubles];
 
-namespace {
-constexpr int kMaxScratchDevices = 64;
-std::mutex g_norm_scratch_mu;
-double* g_norm_scratch_dev[kMaxScratchDevices] = {};
-}  // namespace
-
 // Device address of g_norm_scratch on the current device.  In host code the name
 // g_norm_scratch is only a host-side stand-in, so its address must come from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress with that device current.  It is looked up on every call and
+// not cached: a cached address would outlive a cudaDeviceReset or a change of the
+// current context and point at memory that is no longer the array.  The lookup is a
+// query; only the first one on a device may load the library's module, which is why
+// the first call on a device must come before any stream capture.
 static int norm_scratch_address(double** out) {
     int dev = -1;
     CVFES_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxScratchDevices)
-        return fail(CVFES_ERR_UNSUPPORTED, "cvfes_solid_norms_noalloc_f32: device %d", dev);
-    std::lock_guard<std::mutex> lock(g_norm_scratch_mu);
-    if (!g_norm_scratch_dev[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(CVFES_ERR_CUDA, "cudaGetSymbolAddress(g_norm_scratch) on device %d: %s",
-                        dev, cudaGetErrorString(e));
-        g_norm_scratch_dev[dev] = static_cast<double*>(p);
-    }
-    *out = g_norm_scratch_dev[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(CVFES_ERR_CUDA, "cudaGetSymbolAddress(g_norm_scratch) on device %d: %s", dev,
+                    cudaGetErrorString(e));
+    *out = static_cast<double*>(p);
     return CVFES_OK;
 }
 

@@ -55,7 +55,29 @@ struct StepArgs {
     // polls: the wait gives up with nothing in flight, the kernel records bit 0 in
     // `status` and returns without writing the step.
     int probe_polls = 0;
+    // Fused per-sample norms (persistent fan kernel only; null: off).  Each block keeps
+    // one sample chunk for its whole life and accumulates, per lane and sample, the FP64
+    // sums of u_{n+1}^2, du^2, m du^2 and the non-finite count of u_{n+1} over all its
+    // nodes in shared memory; at its end it writes them to row blockIdx.x / nch of
+    // norm_part [rows][S][4], which k_norms_final then sums in row order.
+    double* norm_part = nullptr;
 };
+
+// Per-lane accumulator of the fused norms: quantity q of sample i of the lane's vector
+// at nacc[(q * V + i) * 32] (lanes innermost: no shared-memory bank conflicts).
+template <typename T, int V>
+__device__ __forceinline__ void norms_add(double* nacc, const Vec<T, V>& im, const double (&su)[V],
+                                          const double (&sv)[V], const double (&nf)[V]) {
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        const double x = (double)im.v[i];
+        const double m = x != 0.0 ? 1.0 / x : 0.0;
+        nacc[(0 * V + i) * 32] += su[i];
+        nacc[(1 * V + i) * 32] += sv[i];
+        nacc[(2 * V + i) * 32] += m * sv[i];
+        nacc[(3 * V + i) * 32] += nf[i];
+    }
+}
 
 // ------------------------------------------------------------ TMA / mbarrier helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -310,22 +332,46 @@ __device__ __forceinline__ void step_update(const StepArgs<T>& A, size_t S, size
 }
 
 // Dirichlet row: u_{n+1} = clamp; in the velocity-state form also v_{n+1} = clamp - u_n.
+// With nacc (fused norms) the row's contributions are added there.
 template <typename T, int V>
-__device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size_t row) {
+__device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size_t row,
+                                            double* nacc = nullptr, long long a = 0,
+                                            size_t col = 0) {
     const Vec<T, V> cl = vfill<T, V>(A.clamp);
+    double su[V], sv[V], nf[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) su[i] = sv[i] = nf[i] = 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        if (A.vel) stcs<T, V>(A.vel + row + d * S, vsub(cl, ldg<T, V>(A.u + row + d * S)));
+        if (A.vel || nacc) {
+            const Vec<T, V> dv = vsub(cl, ldg<T, V>(A.u + row + d * S));
+            if (A.vel) stcs<T, V>(A.vel + row + d * S, dv);
+            if (nacc) {
+#pragma unroll
+                for (int i = 0; i < V; ++i) {
+                    su[i] += (double)cl.v[i] * (double)cl.v[i];
+                    sv[i] += (double)dv.v[i] * (double)dv.v[i];
+                    nf[i] += isfinite(cl.v[i]) ? 0.0 : 1.0;
+                }
+            }
+        }
         stcs<T, V>(A.un + row + d * S, cl);
     }
+    if (nacc) norms_add<T, V>(nacc, ldcs<T, V>(A.invm + (size_t)a * S + col), su, sv, nf);
 }
 
 // As step_update, reading the row's u_{n-1} (or v_n) and inverse mass here.
+// With nacc (fused norms) the row's contributions to the per-sample sums of u_{n+1}^2,
+// du^2 (v_{n+1}^2, or (u_{n+1} - u_n)^2 in FP64) and m du^2 are added there.
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
-                                              const Vec<T, V> (&acc)[3], const T (&f)[3]) {
+                                              const Vec<T, V> (&acc)[3], const T (&f)[3],
+                                              double* nacc = nullptr) {
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
+    double su[V], sv[V], nf[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) su[i] = sv[i] = nf[i] = 0.0;
     if (A.vel) {
         // velocity-state form: v_{n+1} = v_n (1 - eta) + w (p f - K u_n), u_{n+1} = u_n + v_{n+1};
         // a row without mass (u_{n+1} = 0) keeps v_{n+1} = -u_n, the exact increment.
@@ -341,10 +387,16 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
                 const bool live = im.v[i] != T(0);
                 o.v[i] = live ? ua[d].v[i] + v : T(0);
                 vn.v[i] = live ? v : -ua[d].v[i];
+                if (nacc) {
+                    su[i] += (double)o.v[i] * (double)o.v[i];
+                    sv[i] += (double)vn.v[i] * (double)vn.v[i];
+                    nf[i] += isfinite(o.v[i]) ? 0.0 : 1.0;
+                }
             }
             stcs<T, V>(A.un + row + d * S, o);
             stcs<T, V>(A.vel + row + d * S, vn);
         }
+        if (nacc) norms_add<T, V>(nacc, im, su, sv, nf);
         return;
     }
 #pragma unroll
@@ -358,9 +410,16 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
             const T w = A.w0 * im.v[i];
             const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
+            if (nacc) {
+                const double du = (double)o.v[i] - (double)ua[d].v[i];
+                su[i] += (double)o.v[i] * (double)o.v[i];
+                sv[i] += du * du;
+                nf[i] += isfinite(o.v[i]) ? 0.0 : 1.0;
+            }
         }
         stcs<T, V>(A.un + row + d * S, o);
     }
+    if (nacc) norms_add<T, V>(nacc, im, su, sv, nf);
 }
 
 // ------------------------------------------------------------ fan-rotation row
@@ -469,6 +528,72 @@ __device__ __forceinline__ void ku_row_fan(const int4* srec, const T* sslab, int
         fan_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B2, B0, c0, B1, c1);
         if (k >= k1) break;
     }
+}
+
+// ------------------------------------------------------------ fan row, two ahead
+// As ku_row_fan, with each element's new neighbour row and coefficient row requested
+// two elements ahead: four register buffers rotate (first neighbour, second neighbour,
+// and the next two elements' rows in flight), the slot loop unrolled four times.  The
+// products and their order are those of ku_row_fan, so the bits are the same.
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void fan2_phase(int& k, int k1, const int4* srec, const T* sslab,
+                                           const T* __restrict__ u, const T* __restrict__ coef,
+                                           size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                           Vec<T, V> (&acc)[3], Vec<T, V> (&prev)[3],
+                                           Vec<T, V> (&cur)[3], const Vec<T, V>& ccur,
+                                           Vec<T, V> (&n2)[3], Vec<T, V>& c2) {
+    if (k + 2 < k1) {
+        const int4 r2 = srec[k + 2];
+        load_rows<T, V>(n2, u, r2.z, S, col);
+        c2 = ldg<T, V>(coef + (size_t)r2.x * S + col);
+    }
+    to_diff<T, V, DIFF>(cur, ua);
+    slot_fma<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, prev, cur, ua, acc);
+    if (k + 1 < k1) {
+        const int4 r1 = srec[k + 1];
+        if (!(r1.w & 1)) {  // fan break: the next element's first neighbour is new
+            load_rows<T, V>(cur, u, r1.y, S, col);
+            to_diff<T, V, DIFF>(cur, ua);
+        }
+    }
+    ++k;
+}
+
+template <typename T, int V, bool DIFF>
+__device__ __forceinline__ void ku_row_fan2(const int4* srec, const T* sslab, int k0, int k1,
+                                            const T* __restrict__ u, const T* __restrict__ coef,
+                                            size_t S, size_t col, const Vec<T, V> (&ua)[3],
+                                            Vec<T, V> (&acc)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] = vzero<T, V>();
+    if (k0 >= k1) return;
+    Vec<T, V> B0[3], B1[3], B2[3], B3[3], c0, c1, c2, c3;
+    const int4 r0 = srec[k0];
+    load_rows<T, V>(B0, u, r0.y, S, col);
+    load_rows<T, V>(B1, u, r0.z, S, col);
+    c0 = ldg<T, V>(coef + (size_t)r0.x * S + col);
+    if (k0 + 1 < k1) {
+        const int4 r1 = srec[k0 + 1];
+        load_rows<T, V>(B2, u, r1.z, S, col);
+        c1 = ldg<T, V>(coef + (size_t)r1.x * S + col);
+    }
+    to_diff<T, V, DIFF>(B0, ua);
+    int k = k0;
+    while (true) {
+        fan2_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B0, B1, c0, B3, c2);
+        if (k >= k1) break;
+        fan2_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B1, B2, c1, B0, c3);
+        if (k >= k1) break;
+        fan2_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B2, B3, c2, B1, c0);
+        if (k >= k1) break;
+        fan2_phase<T, V, DIFF>(k, k1, srec, sslab, u, coef, S, col, ua, acc, B3, B0, c3, B2, c1);
+        if (k >= k1) break;
+    }
+}
+
+// L1 prefetch of one address (the line lands in L1 and L2; no register is written).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // TMA-tiled step (solid_tile.cu): returns 1 without launching when the mesh has no

@@ -107,6 +107,9 @@ class GPUSolidSolver(PhysicsSolver):
         self.use_graph = getattr(gpu, "use_graph", True)
         self.graph_chunk = getattr(gpu, "graph_chunk", 48)
         self.watchdog = getattr(gpu, "watchdog", True)
+        # norms_every = k > 0: every k-th template step computes the FP64 per-sample norms
+        # of its new state in the same kernel pass (Norms() then returns them)
+        self.norms_every = int(getattr(gpu, "norms_every", 0) or 0)
         # stiffness_update_interval (cvconfig.py:154): 0 keeps the undeformed stiffness and
         # load (linear templates); n >= 1 rebuilds both on x + u every n steps
         self.update_interval = int(getattr(config, "update_interval", 0) or 0)
@@ -206,6 +209,7 @@ class GPUSolidSolver(PhysicsSolver):
             self._graphs = {}
             self._p_buf = None
             self._norm_out = None
+            self._norms_step = -1  # step_count at which _norm_out was fused into a step
             self.step_count = 0
             self.geo_counter = 0
             self.geo_live = False
@@ -291,14 +295,24 @@ class GPUSolidSolver(PhysicsSolver):
             self.step_count += 1
             return
         fn = "cvfes_solid_step_f64" if self.precision == 64 else "cvfes_solid_step_f32"
+        fused = self.norms_every > 0 and (self.step_count + 1) % self.norms_every == 0
+        args = [C_desc(self._desc), ptr(self.plan.coef(self.precision)),
+                ptr(self.plan.invm(self.precision)), ptr(self.bufs[self.cur]),
+                ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), None, None, 0,
+                float(self.pressure), ptr(self.trac_dev), float(dt), float(self.damp)]
         with torch.cuda.device(self.device):
-            call(fn, C_desc(self._desc), ptr(self.plan.coef(self.precision)),
-                 ptr(self.plan.invm(self.precision)), ptr(self.bufs[self.cur]),
-                 ptr(self.bufs[self.prev]), ptr(self.bufs[self.nxt]), None, None, 0,
-                 float(self.pressure), ptr(self.trac_dev), float(dt), float(self.damp),
-                 self._stream())
+            if fused:
+                if self._norm_out is None:
+                    self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
+                                                 device=self.device)
+                call(fn.replace("step_", "step_norms_"), *args, ptr(self.norm_work),
+                     ptr(self._norm_out), 0, self._stream())
+            else:
+                call(fn, *args, self._stream())
         self._rotate()
         self.step_count += 1
+        if fused:
+            self._norms_step = self.step_count
 
     def _rotate(self):
         """Buffer roles after one template step: (u_n, u_{n-1}, free) <- (u_{n+1}, u_n,
@@ -440,21 +454,27 @@ class GPUSolidSolver(PhysicsSolver):
             self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
                                          device=self.device)
         dev_out = self._norm_out
+        fresh = self._norms_step == self.step_count  # fused into the last step
         fn = "cvfes_solid_norms_f64" if self.precision == 64 else "cvfes_solid_norms_f32"
         if self.state_form == "velocity":
             fn = fn.replace("norms_", "norms_vel_")
         chk = self.watchdog if check_finite is None else check_finite
         with torch.cuda.device(self.device):
-            call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
-                 ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
-                 ptr(self.norm_work), ptr(dev_out), int(bool(chk)), self._stream())
+            if not fresh:
+                call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
+                     ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
+                     ptr(self.norm_work), ptr(dev_out), int(bool(chk)), self._stream())
             if out is None:
                 res = dev_out.cpu()
             else:
                 out.copy_(dev_out, non_blocking=True)
                 res = out
             self.plan.check_status()
-        return res.numpy()
+        res = res.numpy()
+        if fresh and chk and np.any(res[:, 3] != 0):
+            raise _lib.NonFiniteError(_lib.CVFES_ERR_NONFINITE,
+                                      "watchdog: %.0f non-finite state values" % res[:, 3].sum())
+        return res
 
     def LambdaMax(self, iters: int = 200, seed: int = 0) -> np.ndarray:
         """Largest eigenvalue of M⁻¹K per sample on the free dofs (FP64 power iteration

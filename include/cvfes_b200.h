@@ -105,6 +105,8 @@ typedef struct cvfes_solid_mesh {
  *               products read shared memory (ids outside the windows read global
  *               memory).  Needs the mesh's tiling (cvfes_mesh_tiles) and S a multiple
  *               of the chunk; otherwise as 3.  vec caps the chunk (vec 1: 32 samples);
+ *           8 = as 3, with each element's rows requested two elements ahead (four
+ *               register buffers rotate instead of three; minb 1..3);
  *   minb: resident blocks per SM the register allocation must allow (1..4).
  * Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t staged,
@@ -119,8 +121,11 @@ int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t
  *             descriptor's bandwidth is 0); 0 = off; else 1..2^20;
  *   parts:    bit 0 = the nodes' state, inverse-mass (and adjoint) rows (contiguous
  *             ranges); bit 1 = the coefficient (and Gamma) rows of their elements,
- *             found through their slot records; -1 (default) = both with at least 4
- *             sample chunks per node block, bit 0 alone below.
+ *             found through their slot records; bit 2 = each warp's own second state
+ *             row and inverse-mass row, read at the end of its node, are prefetched
+ *             into L1 (instead of L2) when the node starts (fan kernels 3 and 8);
+ *             -1 (default) = bits 0 and 1 with at least 4 sample chunks per node
+ *             block, bit 0 alone below.
  * With fewer than 4 sample chunks per node block only every k-th node block
  * prefetches, for k node blocks (k = ceil(4 / chunks)).
  * Results are unchanged; only where the loads hit changes.  Applies to launches
@@ -274,6 +279,28 @@ int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef, const 
                          double pressure, const float* trac, double dt, double damp,
                          void* stream);
 
+/* One step as cvfes_solid_step_* and, in the same pass, the FP64 per-sample norms of the
+ * new state (out f64 [S][4] as cvfes_solid_norms_*: sum u_next^2, sum du^2, sum m du^2,
+ * non-finite count, du = u_next - u, or the new increment in the velocity-state form).
+ * The persistent fan kernel accumulates the sums per block in shared memory while it
+ * writes the state, so the state is not read a second time; shapes without it (S / vec
+ * not a multiple of 32, no max_degree) run the step and the separate norms pass.
+ * work: cvfes_norms_work_size(N, S) doubles.  check_finite: as cvfes_solid_norms_*.
+ * Replaces the reference's per-step host round trip of the state
+ * (physicsSolverSDampGPUs.py:363-390) with one small read-back of per-sample sums.   */
+int cvfes_solid_step_norms_f64(const cvfes_solid_mesh* mesh, const double* coef,
+                               const double* invm, const double* u, const double* u_prev,
+                               double* u_next, const double* p_sched, const int64_t* clock,
+                               int64_t j, double pressure, const double* trac, double dt,
+                               double damp, double* work, double* out, int32_t check_finite,
+                               void* stream);
+int cvfes_solid_step_norms_f32(const cvfes_solid_mesh* mesh, const float* coef,
+                               const float* invm, const float* u, const float* u_prev,
+                               float* u_next, const double* p_sched, const int64_t* clock,
+                               int64_t j, double pressure, const float* trac, double dt,
+                               double damp, double* work, double* out, int32_t check_finite,
+                               void* stream);
+
 /* n_steps steps with the buffer rotation (u_next, u, u_prev) <- (u_prev, u_next, u)
  * of physicsSolverSDampGPUs.py:398-399.  bufs[0] = u_n, bufs[1] = u_{n-1},
  * bufs[2] = free on entry; on return *rot tells which: u_n is bufs[(rot+0)%3]...
@@ -333,9 +360,11 @@ int cvfes_solid_norms_vel_f32(int64_t n_nodes, int64_t n_samples, const float* u
  * whose own pool owns all device memory).  The block partials live in a fixed
  * 4 MiB device array compiled into the library (held on every GPU that loads it
  * until exit), so n_samples may be at most 131071; larger requests fail with
- * CVFES_ERR_ARG.  The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (e.g. on two streams) race.         */
+ * CVFES_ERR_ARG.  Every call looks up that array's device address on the current
+ * device (cudaGetSymbolAddress; nothing is cached, so the address is right after a
+ * device reset too); the first lookup on a device may load the library's module, so
+ * make the first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (e.g. on two streams) race.                          */
 int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples, const float* u,
                                   const float* u_prev, const float* invm, double* out,
                                   int32_t check_finite, void* stream);

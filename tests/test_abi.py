@@ -40,15 +40,21 @@ def test_tuning_setters_validate_and_round_trip(lib):
     try:
         _lib.set_step_prefetch(32, 300, 1)
         assert _lib.get_step_prefetch(32) == dict(distance=300, parts=1)
-        for bad in ((32, -2, 3), (32, (1 << 20) + 1, 3), (16, 4, 3), (32, 4, 4), (32, 4, -2)):
+        for bad in ((32, -2, 3), (32, (1 << 20) + 1, 3), (16, 4, 3), (32, 4, 8), (32, 4, -2)):
             assert lib.cvfes_set_step_prefetch(*bad) == _lib.CVFES_ERR_ARG
             assert "cvfes_set_step_prefetch" in _lib.last_error()
         assert _lib.get_step_prefetch(32) == dict(distance=300, parts=1)
         _lib.set_step_prefetch(32)  # automatic: from the mesh's bandwidth and samples
         assert _lib.get_step_prefetch(32) == dict(distance=-1, parts=-1)
+        _lib.set_step_prefetch(32, 80, 7)  # bit 2: own rows into L1
+        assert _lib.get_step_prefetch(32) == dict(distance=80, parts=7)
+        for bad in ((32, 4, 4, 8, 4), (32, 4, 2, 9, 2), (64, 4, 2, 3, 2)):
+            assert lib.cvfes_set_step_tuning(*bad) == _lib.CVFES_ERR_ARG
+        assert lib.cvfes_set_wait_probe(-1) == _lib.CVFES_ERR_ARG
+        assert lib.cvfes_set_wait_probe(0) == _lib.CVFES_OK
     finally:
         _lib.set_step_prefetch(32, **saved)
     t = _lib.get_step_tuning(64)
     assert lib.cvfes_set_step_tuning(64, 4, 2, 3, 2) == _lib.CVFES_ERR_ARG  # FP64 vec <= 2
-    assert lib.cvfes_set_step_tuning(32, 4, 2, 8, 2) == _lib.CVFES_ERR_ARG  # no variant 8
+    assert lib.cvfes_set_step_tuning(32, 4, 2, 9, 2) == _lib.CVFES_ERR_ARG  # no variant 9
     assert _lib.get_step_tuning(64) == t

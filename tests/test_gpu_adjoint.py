@@ -159,3 +159,20 @@ def test_reverse_kernel_variants_are_bitwise_identical(lib, cuda, precision):
         _lib.set_adjoint_tuning(precision, **saved)
     for tune, (gE, gh) in zip(REV_VARIANTS[precision][1:], outs[1:]):
         assert torch.equal(gE, outs[0][0]) and torch.equal(gh, outs[0][1]), tune
+
+
+def test_autograd_function_flat_fp32_inputs(lib, cuda):
+    """Flat FP32 log E / log h (any shape that reshapes to (E, S)) get gradients of their
+    own shape and dtype."""
+    problem, logE, logh, _ = adjoint_setup(SMALL, precision=64, device=cuda, grad_logh=True)
+    lE = logE.reshape(-1).to(cuda, torch.float32).requires_grad_(True)
+    lh = logh.reshape(-1).to(cuda, torch.float32).requires_grad_(True)
+    J = wall_mismatch(lE, lh, problem)
+    J.sum().backward()
+    assert lE.grad.shape == lE.shape and lE.grad.dtype == torch.float32
+    assert lh.grad.shape == lh.shape and lh.grad.dtype == torch.float32
+    problem.objective(lE.detach().double().reshape(logE.shape),
+                      lh.detach().double().reshape(logh.shape))
+    gE, gh = problem.gradient()
+    assert torch.allclose(lE.grad, gE.reshape(-1).float(), rtol=1e-6, atol=0)
+    assert torch.allclose(lh.grad, gh.reshape(-1).float(), rtol=1e-6, atol=0)

@@ -9,8 +9,10 @@ end of the workload's run: the 256 x 1024 tube after 2000 steps, the stenosed
 
 Here the GPU advances the WHOLE ensemble of each workload with the default kernels
 (FP64 state, and the default FP32 state form) and the chunk's samples are compared:
-relative L2 over the fixture's 2048 nodes, and the per-sample sums over all nodes of
-u^2 (and, for FP64, of the last increment squared).  FP64 <= 1e-12, FP32 <= 1e-5.
+relative L2 over the fixture's 2048 nodes and the per-sample sum over all nodes of
+u^2: FP64 <= 1e-12 (2e-12 for the sum), FP32 <= 1e-5 (2e-5); and for FP64 the sum of
+the last increment squared, <= 1e-9 (the increment is small against u, so its
+relative error is larger).
 """
 import glob
 import os
@@ -100,5 +102,5 @@ def test_full_run_against_reference(lib, cuda, name, precision):
     assert np.all(nrm[:, 3] == 0)
     assert err <= TOL[precision]
     assert e_u2 <= 2 * TOL[precision]
-    if precision == 64:
-        assert e_du2 <= 2 * TOL[precision]
+    if precision == 64:  # the increment is small against u: its relative error is larger
+        assert e_du2 <= 1e-9

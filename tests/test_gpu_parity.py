@@ -29,7 +29,8 @@ class Cfg:
         self.dt = dt
         self.nSmp = nSmp
         self.gpu = type("G", (), dict(precision=precision, use_graph=True, graph_chunk=kw.get("chunk", 6),
-                                      watchdog=True, device=0))()
+                                      watchdog=True, device=0, state=kw.get("state", "auto"),
+                                      norms_every=kw.get("norms_every", 0)))()
         self.dt_f = 0.01
         self.exportBdyStressFilename = None
         self.useConstantStress = False
@@ -208,17 +209,18 @@ def test_invalid_arguments_are_rejected(lib, cuda):
 
 VARIANTS = {32: [(0, 4, 8, 1), (1, 4, 4, 2), (2, 4, 4, 2), (3, 4, 2, 2), (4, 4, 4, 2), (4, 4, 4, 3),
                  (4, 2, 8, 3), (3, 2, 4, 3), (1, 1, 8, 4), (6, 4, 2, 1), (7, 2, 2, 2),
-                 (7, 1, 2, 2)],
+                 (7, 1, 2, 2), (8, 4, 2, 1), (8, 4, 2, 2), (8, 2, 2, 3), (5, 4, 2, 1)],
             64: [(0, 2, 8, 1), (1, 2, 4, 2), (3, 2, 2, 2), (4, 2, 4, 2), (4, 1, 6, 3), (3, 1, 4, 3),
-                 (6, 2, 4, 2), (7, 1, 2, 2)]}
+                 (6, 2, 4, 2), (7, 1, 2, 2), (8, 2, 2, 2), (8, 1, 4, 3)]}
 
 
-@pytest.mark.parametrize("precision", [32, 64])
-def test_step_kernel_variants_are_bitwise_identical(lib, cuda, precision):
+@pytest.mark.parametrize("precision,state", [(32, "previous"), (32, "velocity"),
+                                             (64, "previous"), (64, "velocity")])
+def test_step_kernel_variants_are_bitwise_identical(lib, cuda, precision, state):
     """Every step-kernel variant (L1 gather, TMA-staged, cp.async gather, fan rotation,
-    pipelined persistent, persistent fan, TMA-tiled strips) computes the same
-    floating-point operations in the same order: their states after 60 steps must be
-    bitwise equal."""
+    pipelined persistent, persistent fan, TMA-tiled strips, two-ahead fan, burst gather)
+    computes the same floating-point operations in the same order: their states after
+    60 steps must be bitwise equal, in either state form."""
     from cvfes_b200.cases import CASES
     case = CASES["tube64x128"]
     S = 128 if precision == 32 else 64
@@ -228,7 +230,8 @@ def test_step_kernel_variants_are_bitwise_identical(lib, cuda, precision):
     try:
         for staged, vec, npb, minb in VARIANTS[precision]:
             _lib.set_step_tuning(precision, vec, npb, staged, minb)
-            s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
+            s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12,
+                                                      state=state))
             s.Advance(case.pressures(60))
             s.plan.check_status()
             outs.append(((staged, vec, npb, minb), s.local_displacement().clone()))
@@ -339,7 +342,8 @@ def test_fan_prefetch_distance_leaves_results_unchanged(lib, cuda):
         outs = []
         try:
             _lib.set_step_tuning(precision, vec, 2, 3, 2)
-            for dist, parts in ((0, 0), (1, 3), (80, 1), (80, 2), (-1, -1), (1 << 20, 3)):
+            for dist, parts in ((0, 0), (1, 3), (80, 1), (80, 2), (-1, -1), (1 << 20, 3),
+                                (80, 7), (0, 4)):
                 _lib.set_step_prefetch(precision, dist, parts)
                 s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12))
                 s.Advance(pres)
@@ -531,3 +535,30 @@ def test_geometric_step_tunings_are_bitwise_identical(lib, cuda, precision):
         call("cvfes_set_geo_tuning", precision, saved[0].value, saved[1].value)
     for o in outs[1:]:
         assert torch.equal(o, outs[0])
+
+
+@pytest.mark.parametrize("precision,state,S", [(32, "velocity", 128), (32, "previous", 128),
+                                               (64, "previous", 64), (64, "velocity", 64),
+                                               (32, "velocity", 16)])
+def test_fused_step_norms_match_separate_pass(lib, cuda, precision, state, S):
+    """Solve with the norms fused into the step (persistent fan kernel; with 16 samples
+    the shape has no fused kernel and the step falls back to the separate pass): the
+    state bits of the plain step, and norms equal to the separate pass's to summation-
+    order rounding (1e-13)."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(S)
+    pres = case.pressures(24)
+    plain = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12, state=state))
+    fused = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, S, precision, chunk=12, state=state,
+                                                  norms_every=1))
+    for n in range(24):
+        for s in (plain, fused):
+            s.pressure = float(pres[n])
+            s.Solve(n * case.dt, case.dt)
+        nf, npl = fused.Norms(), plain.Norms()
+        assert fused._norms_step == fused.step_count
+        assert np.all(nf[:, 3] == 0) and np.all(npl[:, 3] == 0)
+        if n > 0:
+            np.testing.assert_allclose(nf[:, :3], npl[:, :3], rtol=1e-13, atol=0)
+    assert torch.equal(fused.local_displacement(), plain.local_displacement())
