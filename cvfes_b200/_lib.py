@@ -56,7 +56,7 @@ class SolidMeshDesc(C.Structure):
         ("tile_pad", C.c_int32),
         ("bandwidth", C.c_int64),
         ("state_form", C.c_int32),
-        ("state_pad", C.c_int32),
+        ("damping_form", C.c_int32),
     ]
 
 

@@ -10,7 +10,7 @@ The config classes keep the reference's attribute names (``cvconfig.py:17-219``)
 and add two optional sections used only by this package:
 
 * ``[gpu]``: ``precision`` (fp64 | fp32), ``state`` (auto | previous | velocity),
-  ``use_graph``, ``graph_chunk``,
+  ``semantics`` (cpu | opencl), ``use_graph``, ``graph_chunk``,
   ``norms_every``, ``watchdog``, ``device``;
 * ``[synthetic]``: a structured tube wall mesh with GMRF material samples in
   place of the VTP files the reference reads (see :mod:`cvfes_b200.cases`).
@@ -249,6 +249,11 @@ class GPUConfig:
         self.state = sec.get_str("state", "auto").lower()
         if self.state not in ("auto", "previous", "velocity"):
             raise ValueError("[gpu] state must be auto, previous or velocity")
+        # numerics of the step: cpu (SolidSolver, physicsSolver.py) or opencl (the
+        # OpenCL class the drop-in replaces, physicsSolverSDampGPUs.py/.cl)
+        self.semantics = sec.get_str("semantics", "cpu").lower()
+        if self.semantics not in ("cpu", "opencl"):
+            raise ValueError("[gpu] semantics must be cpu or opencl")
 
 
 class CVConfig:

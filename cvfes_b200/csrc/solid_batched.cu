@@ -49,6 +49,7 @@ struct BatchMesh {
     int npb;     // nodes per block
     int chunks;  // sample chunks per node block (the last one may be partial)
     int form;    // 1: velocity-state form (buf[1] holds the increment), 0: u_{n-1} in buf
+    int damp_dof;  // 1: damping per dof (eta = dt damp / m per row), 0: mass-proportional
     // fan kernel layout: items of kBatchWarps warps, f_npw nodes per warp
     long long f_off;  // first fan item of this mesh
     int f_tpn;        // lanes per node (min(32, S/VEC))
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restric
         A.clamp = (T)M.clamp;
         A.eta = (T)M.eta;
         A.w0 = (T)M.w0;
+        A.damp_per_dof = M.damp_dof;
         const size_t S = (size_t)M.S;
         const size_t col = (size_t)vec * V;
         const size_t row = (size_t)a * 3 * S + col;
@@ -230,6 +232,7 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
         A.clamp = (T)M.clamp;
         A.eta = (T)M.eta;
         A.w0 = (T)M.w0;
+        A.damp_per_dof = M.damp_dof;
         const size_t S = (size_t)M.S;
         const size_t col = (size_t)vec * V;
         const size_t row = (size_t)a * 3 * S + col;
@@ -393,8 +396,11 @@ extern "C" int cvfes_batch_pack(const cvfes_batch_item* items, int32_t n_meshes,
         b.n_clamped = (int)ms.n_clamped;
         b.clamp = ms.clamp_value;
         const double g = 0.5 * it.dt * it.damp;
-        b.eta = it.dt * it.damp / (1.0 + g);
-        b.w0 = it.dt * it.dt / (1.0 + g);
+        if (ms.damping_form != 0 && ms.damping_form != 1)
+            return fail(CVFES_ERR_ARG, "cvfes_batch_pack: mesh %d damping_form", m);
+        b.damp_dof = ms.damping_form;
+        b.eta = b.damp_dof ? it.dt * it.damp : it.dt * it.damp / (1.0 + g);
+        b.w0 = b.damp_dof ? it.dt * it.dt : it.dt * it.dt / (1.0 + g);
         const int sv = (int)(ms.n_samples / vec);
         b.tpn = sv < 32 ? sv : 32;
         b.npb = 256 / b.tpn;

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(256) k_step_geo(StepArgs<T> A, GeoArgs<T> G) {
             const T w = A.w0 * im.v[i];
             T f = p * load[i][d];
             if (A.trac) f += tr;
-            const T v = fma(w, f - acc[i][d], fma(-A.eta, dv, dv));
+            const T v = fma(w, f - acc[i][d], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
         }
         stcs<T, V>(A.un + row + d * S, o);
@@ -299,8 +299,14 @@ int launch_step_geo(const cvfes_solid_mesh* m, const T* coef, const T* invm, con
     A.n_clamped = (int)m->n_clamped;
     A.clamp = (T)m->clamp_value;
     const double g = 0.5 * dt * damp;
-    A.eta = (T)(dt * damp / (1.0 + g));
-    A.w0 = (T)(dt * dt / (1.0 + g));
+    if (m->damping_form == 1) {  // damping force per dof: eta = dt damp / m, no LHS term
+        A.damp_per_dof = 1;
+        A.eta = (T)(dt * damp);
+        A.w0 = (T)(dt * dt);
+    } else {
+        A.eta = (T)(dt * damp / (1.0 + g));
+        A.w0 = (T)(dt * dt / (1.0 + g));
+    }
     A.status = m->status;
     GeoArgs<T> G;
     G.geo = geo;

@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// u_prev = u0 - dt du0 + dt^2/2 ddu0, ddu0 = (p0 f - damp m du0 - K u0)/m  (0 where m == 0);
+// u_prev = u0 - dt du0 + dt^2/2 ddu0, ddu0 = (p0 f - damp m du0 - K u0)/m  (0 where m == 0;
+// the launcher passes damp = 0 for damping per dof, whose calc_ddu has no damping term);
 // in the velocity-state form (vel) the increment u0 - u_prev = dt du0 - dt^2/2 ddu0 instead.
 template <typename T>
 __global__ void k_init(const T* fhat, const T* invm, const T* u0, const T* du0, const T* ku,
@@ -231,7 +232,7 @@ __global__ void k_init(const T* fhat, const T* invm, const T* u0, const T* du0, 
     for (int d = 0; d < 3; ++d) {
         const size_t o = ((size_t)a * 3 + d) * S + s;
         const T m = im != T(0) ? T(1) / im : T(0);
-        const T rhs = p0 * fhat[4 * a + d] - damp * m * du0[o] - ku[o];
+        const T rhs = p0 * fhat[4 * a + d] - damp * m * du0[o] - ku[o];  // damp = 0: per dof
         const T acc = im != T(0) ? rhs * im : T(0);
         u_prev[o] = vel ? dt * du0[o] - T(0.5) * dt * dt * acc
                         : u0[o] - dt * du0[o] + T(0.5) * dt * dt * acc;
@@ -758,7 +759,7 @@ __global__ void __launch_bounds__(256, 1) k_step_pipe(PipeArgs<T> P) {
                 for (int i = 0; i < V; ++i) {
                     const T dv = ua[d].v[i] - up.v[i];
                     const T w = A.w0 * im.v[i];
-                    const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+                    const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
                     o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
                 }
                 stcs<T, V>(A.un + row + d * S, o);
@@ -934,7 +935,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_gather(StepArgs<T> A) {
         for (int i = 0; i < V; ++i) {
             const T dv = ua[d].v[i] - up.v[i];
             const T w = A.w0 * im.v[i];
-            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
         }
         stcs<T, V>(A.un + row + d * S, o);
@@ -1259,8 +1260,16 @@ int launch_step(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     A.n_clamped = (int)m->n_clamped;
     A.clamp = (T)m->clamp_value;
     const double g = 0.5 * dt * damp;
-    A.eta = (T)(dt * damp / (1.0 + g));
-    A.w0 = (T)(dt * dt / (1.0 + g));
+    if (m->damping_form != 0 && m->damping_form != 1)
+        return fail(CVFES_ERR_ARG, "cvfes_solid_step: damping_form must be 0 or 1");
+    if (m->damping_form == 1) {  // damping force per dof: eta = dt damp / m, no LHS term
+        A.damp_per_dof = 1;
+        A.eta = (T)(dt * damp);
+        A.w0 = (T)(dt * dt);
+    } else {
+        A.eta = (T)(dt * damp / (1.0 + g));
+        A.w0 = (T)(dt * dt / (1.0 + g));
+    }
     A.status = m->status;
     A.cap_slots = 0;
     if (m->state_form != 0 && m->state_form != 1)
@@ -1463,7 +1472,7 @@ int launch_init(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T
     const int block = 256;
     k_init<T><<<grid_1d(m->n_nodes * S, block), block, 0, st>>>(
         static_cast<const T*>(m->fhat), invm, u0, du0, work, u_prev, m->n_nodes, S, (T)p0, (T)dt,
-        (T)damp, m->state_form == 1 ? 1 : 0);
+        (T)(m->damping_form == 1 ? 0.0 : damp), m->state_form == 1 ? 1 : 0);
     CVFES_LAUNCH_CHECK("k_init");
     return CVFES_OK;
 }

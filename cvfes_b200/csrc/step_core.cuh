@@ -61,7 +61,16 @@ struct StepArgs {
     // nodes in shared memory; at its end it writes them to row blockIdx.x / nch of
     // norm_part [rows][S][4], which k_norms_final then sums in row order.
     double* norm_part = nullptr;
+    // Damping per dof (the OpenCL class's calc_u): eta = dt damp / m per row, w = dt^2 / m.
+    // Off: mass-proportional damping, one eta for all rows.  Set: A.eta holds dt damp.
+    int damp_per_dof = 0;
 };
+
+// eta of one row: dt damp / m (damping per dof) or the launch's eta.
+template <typename T>
+__device__ __forceinline__ T row_eta(const StepArgs<T>& A, T im) {
+    return A.damp_per_dof ? A.eta * im : A.eta;
+}
 
 // Per-lane accumulator of the fused norms: quantity q of sample i of the lane's vector
 // at nacc[(q * V + i) * 32] (lanes innermost: no shared-memory bank conflicts).
@@ -324,7 +333,7 @@ __device__ __forceinline__ void step_update(const StepArgs<T>& A, size_t S, size
         for (int i = 0; i < V; ++i) {
             const T dv = ua[d].v[i] - up.v[i];
             const T w = A.w0 * im.v[i];
-            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
         }
         stcs<T, V>(A.un + row + d * S, o);
@@ -383,7 +392,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
 #pragma unroll
             for (int i = 0; i < V; ++i) {
                 const T w = A.w0 * im.v[i];
-                const T v = fma(w, load - acc[d].v[i], fma(-A.eta, vo.v[i], vo.v[i]));
+                const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), vo.v[i], vo.v[i]));
                 const bool live = im.v[i] != T(0);
                 o.v[i] = live ? ua[d].v[i] + v : T(0);
                 vn.v[i] = live ? v : -ua[d].v[i];
@@ -408,7 +417,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
         for (int i = 0; i < V; ++i) {
             const T dv = ua[d].v[i] - up.v[i];
             const T w = A.w0 * im.v[i];
-            const T v = fma(w, load - acc[d].v[i], fma(-A.eta, dv, dv));
+            const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
             if (nacc) {
                 const double du = (double)o.v[i] - (double)ua[d].v[i];

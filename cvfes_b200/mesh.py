@@ -211,6 +211,23 @@ class SolidMesh:
         coefK = np.ascontiguousarray((gH * gE) @ wt)
         return coefK, gH
 
+    # -- the OpenCL class's material, physicsSolverSDampGPUs.py:160-175 --
+    def opencl_coefficients(self):
+        """Return ``(elmTE (E,S), nodal thickness at the element's nodes (E,S,3))`` as the
+        OpenCL solver class builds them: the stiffness coefficient is the mean over the
+        element's three nodes of ``E * h`` (``physicsSolverSDampGPUs.py:166-175``) and the
+        mass uses the thickness of each node (``assemble_K_M_P``,
+        ``physicsSolverSDampGPUs.cl:174-223``).  Per-element fields are constant over the
+        element's nodes."""
+        if self.vE is not None and self.coefK is None and self.elmE is None:
+            ve = np.asarray(self.vE, dtype=np.float64)[self.elementNodeIds, :]       # (E,3,S)
+            vh = np.asarray(self.vthickness, dtype=np.float64)[self.elementNodeIds, :]
+            elm_te = np.ascontiguousarray((ve * vh).mean(axis=1))
+            return elm_te, np.ascontiguousarray(vh.swapaxes(1, 2))
+        coefK, gthick = self.element_coefficients()
+        h = gthick.mean(axis=2) if gthick.ndim == 3 else gthick
+        return coefK, np.ascontiguousarray(np.repeat(h[:, :, None], 3, axis=2))
+
     def element_moduli(self):
         """Young's modulus per element and sample (E,S): the mean over the three quadrature
         points, as the stress recovery uses it (``physicsSolver.py:416-424``).  With only

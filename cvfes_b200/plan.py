@@ -47,10 +47,19 @@ def lumped_mass_weights(density: float, lumping: str = "reference") -> np.ndarra
     ``w_g`` a second time, optimizedSolidAssemble.pyx:564-566), one third of
     the element mass per node.
     ``rowsum``: ``rho * w_g * N_g(a)`` -- the row sum of the consistent mass
-    matrix (the full rho*h*A/3 per node); equal to ``reference`` with 3 rho."""
+    matrix (the full rho*h*A/3 per node); equal to ``reference`` with 3 rho.
+    ``opencl``: the OpenCL class's lumping of nodal thickness (``assemble_K_M_P``,
+    physicsSolverSDampGPUs.cl:174-223): node a gets ``rho A/3 sum_k W[a][k] h_k``
+    with ``h_k`` the thickness of the element's node k; its rows are the sums of the
+    kernel's ab terms, row 2 with the kernel's own ``ab = 22`` weights (h1/4, not h2/4,
+    physicsSolverSDampGPUs.cl:218), so W[2] = (1/4, 3/8, 3/8).  With one thickness per
+    element every row sums to rho h A/3, the ``rowsum`` mass."""
+    if lumping == "opencl":
+        W = np.array([[0.5, 0.25, 0.25], [0.25, 0.5, 0.25], [0.25, 0.375, 0.375]])
+        return density * W / 3.0
     w = QUAD[:, 3:4] ** 2 if lumping == "reference" else QUAD[:, 3:4]
     if lumping not in ("reference", "rowsum"):
-        raise ValueError("mass lumping must be 'reference' or 'rowsum'")
+        raise ValueError("mass lumping must be 'reference', 'rowsum' or 'opencl'")
     return density * (QUAD[:, :3] * w).T.copy()
 
 

@@ -22,7 +22,14 @@ Differences by design:
 * FP64 (default) or FP32 state, chosen by ``[gpu] precision``;
 * the second state buffer holds u_{n-1} as in the reference, or (``[gpu] state``
   velocity, the default for the FP32 state) the increment v_n = u_n - u_{n-1},
-  updated in place, so the FP32 rounding of u is not fed back into the velocity.
+  updated in place, so the FP32 rounding of u is not fed back into the velocity;
+* the numerics are those of the reference's CPU SolidSolver (``[gpu] semantics`` cpu,
+  the default) or of the OpenCL class this one replaces (opencl): stiffness
+  coefficient mean(E h) over the element's nodes, its lumping of nodal thickness,
+  damping force -damp (u - u_prev)/dt per dof with LM on the left-hand side, no
+  damping in the start-up acceleration, stiffness and follower pressure rebuilt on
+  x + u every step (``physicsSolverSDampGPUs.py:160-175, 325-399``,
+  ``physicsSolverSDampGPUs.cl:174-223, 398-429``).
 """
 from __future__ import annotations
 
@@ -113,6 +120,14 @@ class GPUSolidSolver(PhysicsSolver):
         # stiffness_update_interval (cvconfig.py:154): 0 keeps the undeformed stiffness and
         # load (linear templates); n >= 1 rebuilds both on x + u every n steps
         self.update_interval = int(getattr(config, "update_interval", 0) or 0)
+        # semantics: cpu (SolidSolver's numerics) or opencl (the numerics of the OpenCL class
+        # physicsSolverSDampGPUs.py, which rebuilds the stiffness and the follower pressure
+        # on x + u every step, so its stiffness update interval is 1)
+        self.semantics = str(getattr(gpu, "semantics", "cpu") or "cpu").lower()
+        if self.semantics not in ("cpu", "opencl"):
+            raise ValueError("semantics must be cpu or opencl")
+        if self.semantics == "opencl":
+            self.update_interval = 1
         self.state_form = resolve_state_form(getattr(gpu, "state", "auto"), self.precision,
                                              self.update_interval)
         self.InitializeSync()
@@ -180,11 +195,13 @@ class GPUSolidSolver(PhysicsSolver):
         m = self.mesh
         dev = self.device
         with torch.cuda.device(dev):
+            opencl = self.semantics == "opencl"
+            lumping = "opencl" if opencl else getattr(m, "mass_lumping", "reference")
             self.plan = SolidPlan(m.nodes[self.lclNodeIds], self.lclElmNodeIds,
                                   n_clamped=m.lclNSpecialHead, clamp_value=m.bdyU, v=m.v,
                                   density=m.density, device=dev, precisions=(self.precision,),
-                                  mass_lumping=getattr(m, "mass_lumping", "reference"))
-            coefK, gthick = m.element_coefficients()
+                                  mass_lumping=lumping)
+            coefK, gthick = m.opencl_coefficients() if opencl else m.element_coefficients()
             self.plan.set_material(coefK, gthick)
             self.refresh_desc()
             dtype = torch.float64 if self.precision == 64 else torch.float32
@@ -232,6 +249,7 @@ class GPUSolidSolver(PhysicsSolver):
         arrays change), with this solver's state form."""
         self._desc = self.plan.desc(self.precision)
         self._desc.state_form = 1 if self.state_form == "velocity" else 0
+        self._desc.damping_form = 1 if self.semantics == "opencl" else 0
         return self._desc
 
     # ------------------------------------------------------------------ per step

@@ -76,7 +76,13 @@ typedef struct cvfes_solid_mesh {
                                      holds: 0 = u_{n-1} (the reference's pair of
                                      displacements), 1 = the increment v_n = u_n - u_{n-1},
                                      updated in place by each step (velocity-state form) */
-    int32_t        state_pad;
+    int32_t        damping_form;  /* 0 = mass-proportional damping LC = damp * LM and the
+                                     left-hand side LM + dt/2 LC (SolidSolver,
+                                     physicsSolver.py:263-292); 1 = damping force
+                                     -damp (u - u_prev) / dt per dof and the left-hand
+                                     side LM, with no damping in the start-up
+                                     acceleration (the OpenCL class's calc_u and
+                                     calc_ddu, physicsSolverSDampGPUs.cl:398-429) */
 } cvfes_solid_mesh;
 
 /* Step-kernel tuning (the autotuner sets these; defaults: variant 3, FP32 vec 4,

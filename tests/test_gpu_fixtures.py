@@ -4,11 +4,12 @@
 ensemble, the state the reference's CPU solid path (its compiled assembly and
 ``MultiplyByVector`` with the update of ``physicsSolver.py:263-292``) reached at the
 end of the workload's run: the 256 x 1024 tube after 2000 steps, the stenosed
-512 x 2048 tube after 1000 steps and four tubes of the uneven 64-tube ensemble after
+512 x 2048 tube after 1000 steps and five tubes of the uneven 64-tube ensemble after
 1000 steps (``tests/golden/make_full_fixtures.py``).
 
 Here the GPU advances the WHOLE ensemble of each workload with the default kernels
-(FP64 state, and the default FP32 state form) and the chunk's samples are compared:
+(FP64 state, and the default FP32 state form; the batch tubes through the batched
+kernels) and the chunk's samples are compared:
 relative L2 over the fixture's 2048 nodes and the per-sample sum over all nodes of
 u^2: FP64 <= 1e-12 (2e-12 for the sum), FP32 <= 1e-5 (2e-5); and for FP64 the sum of
 the last increment squared, <= 1e-9 (the increment is small against u, so its
@@ -21,6 +22,7 @@ import numpy as np
 import pytest
 import torch
 
+from cvfes_b200.batched import BatchedSolidSolver
 from cvfes_b200.cases import CASES, batched_cases, build_mesh, case_dt
 from cvfes_b200.solver import GPUSolidSolver, LocalComm
 
@@ -82,8 +84,14 @@ def test_full_run_against_reference(lib, cuda, name, precision):
     coefK, gthick = mesh.element_coefficients()
     chk = material_checksum(coefK[:, idx], gthick[:, idx])
     assert np.allclose(chk, fx["material"], rtol=1e-12, atol=0), "material differs"
-    s = GPUSolidSolver(LocalComm(), mesh, Cfg(dt, mesh.nSmp, precision))
-    s.Advance(case.pressures(int(fx["n_steps"])))
+    if name.startswith("batch"):  # the batched kernels (a batch of this one tube)
+        batch = BatchedSolidSolver([mesh], [dt], precision=precision, device=cuda)
+        batch.Advance(case.pressures(int(fx["n_steps"])))
+        batch.release_graphs()
+        s = batch.solvers[0]
+    else:
+        s = GPUSolidSolver(LocalComm(), mesh, Cfg(dt, mesh.nSmp, precision))
+        s.Advance(case.pressures(int(fx["n_steps"])))
     nrm = s.Norms()
     inv = np.empty(s.lclNDof, dtype=np.int64)
     inv[s.dofs] = np.arange(s.lclNDof)

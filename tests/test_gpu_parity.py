@@ -30,7 +30,8 @@ class Cfg:
         self.nSmp = nSmp
         self.gpu = type("G", (), dict(precision=precision, use_graph=True, graph_chunk=kw.get("chunk", 6),
                                       watchdog=True, device=0, state=kw.get("state", "auto"),
-                                      norms_every=kw.get("norms_every", 0)))()
+                                      norms_every=kw.get("norms_every", 0),
+                                      semantics=kw.get("semantics", "cpu")))()
         self.dt_f = 0.01
         self.exportBdyStressFilename = None
         self.useConstantStress = False
@@ -562,3 +563,36 @@ def test_fused_step_norms_match_separate_pass(lib, cuda, precision, state, S):
         if n > 0:
             np.testing.assert_allclose(nf[:, :3], npl[:, :3], rtol=1e-13, atol=0)
     assert torch.equal(fused.local_displacement(), plain.local_displacement())
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_opencl_semantics_against_restatement(lib, cuda, precision):
+    """[gpu] semantics = opencl (the OpenCL class's numerics: mean(E h) over the element's
+    nodes, its lumping of nodal thickness, damping force per dof with LHS = LM, no damping
+    in the start-up acceleration, stiffness and follower pressure on x + u every step)
+    against the NumPy restatement of its kernels, with nodal material that varies node
+    by node and damping 100: FP64 <= 1e-12, FP32 <= 1e-5 at every 10th step."""
+    from cvfes_b200.mesh import TubeGeometry, tube_mesh
+    from oracle.opencl_oracle import OpenCLSolidOracle
+    nodes, elems, inl, outl = tube_mesh(TubeGeometry(16, 12, 3.0, 0.3))
+    bdy = np.concatenate([inl, outl])
+    N, S = len(nodes), 4
+    rng = np.random.default_rng(11)
+    vE = 7e6 * np.exp(0.2 * rng.standard_normal((N, S)))
+    vh = 0.04 * np.exp(0.1 * rng.standard_normal((N, S)))
+    dt, damp = 2e-6, 100.0
+    mesh = SolidMesh(nodes, elems, bdy, S, density=1.0, v=0.49, damp=damp, vE=vE, vthickness=vh)
+    ocl = OpenCLSolidOracle(nodes, elems, bdy, vE, vh, 1.0, 0.49, damp, dt)
+    s = GPUSolidSolver(LocalComm(), mesh, Cfg(dt, S, precision, chunk=12, semantics="opencl"))
+    assert s.update_interval == 1 and s._desc.damping_form == 1
+    pres = 1.33e5 * np.minimum(np.arange(40) / 10.0, 1.0)
+    tol = FP64_TOL if precision == 64 else FP32_TOL
+    worst = 0.0
+    for n, p in enumerate(pres):
+        s.pressure = float(p)
+        s.Solve(n * dt, dt)
+        ref = ocl.step(p)
+        if (n + 1) % 10 == 0:
+            worst = max(worst, so.rel_l2(s.displacement(), ref))
+    print(f"opencl semantics FP{precision}: max rel-L2 {worst:.3e}")
+    assert np.abs(ref).max() > 0 and worst < tol
