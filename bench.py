@@ -274,6 +274,11 @@ def gpu_main(args, case, rank, world, local, dev):
     Cfg.constant_T = RAMP_STEPS * dt
 
     solver = GPUSolidSolver(LocalComm(), mesh, Cfg)
+    from cvfes_b200 import _lib
+    variant = _lib.get_step_tuning(prec)["staged"]
+    kernel = {0: "k_step", 1: "k_step_staged", 2: "k_step_gather", 3: "k_step_fan",
+              4: "k_step_pipe", 5: "k_step_burst", 6: "k_step_fanp", 7: "k_step_tile",
+              8: "k_step_fan (two ahead)"}.get(variant, str(variant))
     K, W = args.steps, args.warmup
     pres = torch.from_numpy(case.pressures(W + K)).to(dev)
     stream = torch.cuda.current_stream(dev)
@@ -351,7 +356,7 @@ def gpu_main(args, case, rank, world, local, dev):
                          " (norms fused into the step kernel)"),
                 "h2d_bytes_per_step": 8, "d2h_bytes_per_step": S * 4 * 8 + 8},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_step_fan", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "traffic": traffic, "peak_source": peak_kind, "bytes_per_step": bstep},
         "clocks": ck,

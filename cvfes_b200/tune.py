@@ -22,9 +22,10 @@ import torch
 from . import _lib
 
 STEP_CANDIDATES = {
-    32: [(3, 4, 2, 2), (3, 4, 4, 2), (3, 4, 2, 1), (1, 4, 4, 2), (3, 2, 2, 3), (5, 4, 2, 1),
-         (0, 4, 8, 1)],
-    64: [(3, 2, 2, 2), (3, 2, 4, 2), (1, 2, 4, 2), (3, 1, 4, 3), (5, 1, 2, 2), (0, 2, 8, 1)],
+    32: [(6, 4, 2, 2), (6, 4, 4, 2), (3, 4, 2, 2), (3, 4, 4, 2), (8, 4, 2, 2), (3, 4, 2, 1),
+         (1, 4, 4, 2), (3, 2, 2, 3), (5, 4, 2, 1), (0, 4, 8, 1)],
+    64: [(3, 2, 2, 2), (3, 2, 4, 2), (6, 2, 2, 2), (8, 2, 2, 2), (1, 2, 4, 2), (3, 1, 4, 3),
+         (5, 1, 2, 2), (0, 2, 8, 1)],
 }
 
 
@@ -109,7 +110,7 @@ def tune_step(solver, candidates: Optional[Iterable[Tuple[int, int, int, int]]] 
                                  ms_per_step=ms)))
     best = min(results, key=lambda r: r[0])[1]
     _lib.set_step_tuning(prec, best["vec"], best["npb"], best["staged"], best["minb"])
-    if best["staged"] == 3:
+    if best["staged"] in (3, 6, 8):
         bw = solver.plan.bandwidth
         for pf in (dict(distance=0, parts=0), dict(distance=-1, parts=1),
                    dict(distance=-1, parts=3), dict(distance=2 * bw + 128, parts=3)):
