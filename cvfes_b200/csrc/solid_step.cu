@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -419,6 +420,8 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
             prefetch_l2(A.invm + (size_t)a * S + col);
             node_load<T>(A, a, p, f);
         }
+        if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
+            fan_prefetch(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
         if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
             if (lane == 0 && A.status) atomicOr(A.status, 1);
             return;
@@ -982,16 +985,41 @@ __global__ void k_norms_partial(long long n_nodes, int S, long long npc, const T
     w[3] = nf;
 }
 
-__global__ void k_norms_final(long long n_chunks, int S, const double* __restrict__ work,
-                              double* __restrict__ out, double* __restrict__ total_nonfinite) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * S) return;
-    const int s = t / 4, q = t % 4;
+// Sums of the partial rows per (sample, quantity): a block owns kFinalPairs consecutive
+// (sample, quantity) pairs (coalesced across its lanes) and kFinalGroups row groups;
+// group g adds rows g, g + kFinalGroups, ... into four accumulators, and the groups'
+// sums are added in group order, so the result depends only on the row count.
+constexpr int kFinalPairs = 32, kFinalGroups = 8;
+__global__ void __launch_bounds__(kFinalPairs * kFinalGroups)
+    k_norms_final(long long n_chunks, int S, const double* __restrict__ work,
+                  double* __restrict__ out, double* __restrict__ total_nonfinite) {
+    __shared__ double part[kFinalGroups][kFinalPairs];
+    const int lp = threadIdx.x % kFinalPairs, g = threadIdx.x / kFinalPairs;
+    const long long t = (long long)blockIdx.x * kFinalPairs + lp;  // pair s * 4 + q
+    const long long P = 4LL * S;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (t < P) {
+        long long c = g;
+        const size_t stride = (size_t)kFinalGroups * P;
+        const double* w = work + (size_t)c * P + t;
+        for (; c + 3 * kFinalGroups < n_chunks; c += 4 * kFinalGroups, w += 4 * stride) {
+            a0 += w[0];
+            a1 += w[stride];
+            a2 += w[2 * stride];
+            a3 += w[3 * stride];
+        }
+        for (; c < n_chunks; c += kFinalGroups, w += stride) a0 += w[0];
+    }
+    part[g][lp] = (a0 + a1) + (a2 + a3);
+    __syncthreads();
+    if (g != 0 || t >= P) return;
     double acc = 0.0;
-    for (long long c = 0; c < n_chunks; ++c) acc += work[((size_t)c * S + s) * 4 + q];
-    out[(size_t)s * 4 + q] = acc;
-    if (q == 3 && acc != 0.0) atomicAdd(total_nonfinite, acc);
+#pragma unroll
+    for (int k = 0; k < kFinalGroups; ++k) acc += part[k][lp];
+    out[t] = acc;
+    if ((t & 3) == 3 && acc != 0.0) atomicAdd(total_nonfinite, acc);
 }
+inline unsigned final_grid(long long S) { return grid_1d(4 * S, kFinalPairs); }
 
 // ------------------------------------------------------------------ launchers
 template <typename T>
@@ -1120,23 +1148,53 @@ int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, 
     }
 }
 
-// The persistent fan kernel on as many blocks as are resident (at most one per work
-// item).  With fused norms the grid is rounded down to a multiple of the sample chunks
-// and capped at max_rows chunks' worth, and *rows gets the partial rows written.
-template <typename K, typename T>
-int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStream_t st,
-                  const StepArgs<T>& A, long long max_rows, long long* rows) {
+// Resident blocks per SM of a persistent kernel at this block size and shared memory,
+// with the shared-memory attribute set when it needs more than 48 KB; looked up once
+// per (kernel, device, block, shared memory) and kept, since every step launches it.
+int fanp_blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm) {
+    struct Entry {
+        const void* k;
+        int dev, threads;
+        size_t smem;
+        int per_sm;
+    };
+    static Entry cache[32];
+    static int n_cache = 0;
+    static std::mutex mu;
+    int dev = 0;
+    CVFES_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    for (int i = 0; i < n_cache; ++i)
+        if (cache[i].k == kernel && cache[i].dev == dev && cache[i].threads == threads &&
+            cache[i].smem == smem) {
+            *per_sm = cache[i].per_sm;
+            return CVFES_OK;
+        }
     if (smem > 48 * 1024) {
         cudaError_t e =
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess)
             return fail(CVFES_ERR_CUDA, "k_step_fanp smem attribute: %s", cudaGetErrorString(e));
     }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
-            cudaSuccess ||
-        per_sm <= 0)
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess ||
+        n <= 0)
         return fail(CVFES_ERR_CUDA, "k_step_fanp: no resident block fits");
+    if (n_cache < 32) cache[n_cache++] = Entry{kernel, dev, threads, smem, n};
+    *per_sm = n;
+    return CVFES_OK;
+}
+
+// The persistent fan kernel on as many blocks as are resident (at most one per work
+// item).  With fused norms the grid is rounded down to a multiple of the sample chunks
+// and capped at max_rows chunks' worth, and *rows gets the partial rows written.
+template <typename K, typename T>
+int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStream_t st,
+                  const StepArgs<T>& A, long long max_rows, long long* rows) {
+    int per_sm = 0;
+    const int rc = fanp_blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem,
+                                      &per_sm);
+    if (rc) return rc;
     long long blocks = (long long)per_sm * sm_count();
     if (blocks > n_items) blocks = n_items;
     if (A.norm_part) {
@@ -1496,7 +1554,7 @@ int launch_norms(long long n_nodes, long long S, const T* u, const T* up, const 
         k_norms_partial<T, false><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, up, invm,
                                                                  work);
     CVFES_LAUNCH_CHECK("k_norms_partial");
-    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
+    k_norms_final<<<final_grid(S), kFinalPairs * kFinalGroups, 0, st>>>(nch, (int)S, work, out, total);
     CVFES_LAUNCH_CHECK("k_norms_final");
     if (check_finite) {
         double h = 0.0;
@@ -1563,7 +1621,7 @@ int launch_step_norms(const cvfes_solid_mesh* m, const T* coef, const T* invm, c
         return launch_norms<T>(N, S, un, vel ? up : u, invm, work, out, check_finite, st, vel);
     double* total = work + (size_t)rows * S * 4;
     CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
-    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(rows, (int)S, work, out, total);
+    k_norms_final<<<final_grid(S), kFinalPairs * kFinalGroups, 0, st>>>(rows, (int)S, work, out, total);
     CVFES_LAUNCH_CHECK("k_norms_final");
     if (check_finite) {
         double h = 0.0;
@@ -1879,7 +1937,7 @@ extern "C" int cvfes_solid_norms_noalloc_f32(int64_t n_nodes, int64_t n_samples,
     k_norms_partial<float, false><<<grid, kNormThreads, 0, st>>>(n_nodes, (int)S, npc, u, u_prev,
                                                                  invm, work);
     CVFES_LAUNCH_CHECK("k_norms_partial (fixed scratch)");
-    k_norms_final<<<grid_1d(4 * S, 256), 256, 0, st>>>(nch, (int)S, work, out, total);
+    k_norms_final<<<final_grid(S), kFinalPairs * kFinalGroups, 0, st>>>(nch, (int)S, work, out, total);
     CVFES_LAUNCH_CHECK("k_norms_final (fixed scratch)");
     if (check_finite) {
         double h = 0.0;
