@@ -607,6 +607,130 @@ __global__ void __launch_bounds__(256, MINB) k_reverse_fan(RevArgs<T> A) {
     rev_epilogue<T, V, GM>(A, a, S, col, row, ua, ca, accU, accC);
 }
 
+// ------------------------------------------------------------ persistent reverse step
+// k_reverse_fan as a persistent grid: each block walks work items (node block, sample
+// chunk; chunk fastest) with a stride of the grid and stages the slot records,
+// stiffness rows and owner blocks of its NEXT item by TMA into the other of two
+// shared-memory stages while its warps run the current one.  Stage s of the block's
+// i-th item completes its mbarrier's phase (i / 2) % 2; a block barrier at the end of
+// every item frees the stage for reuse.  Same products in the same order: same bits.
+template <typename T>
+__device__ __forceinline__ void revp_issue(const RevArgs<T>& A, long long w, uint32_t bar,
+                                           int4* srec, T* sslab, T* sown) {
+    const long long nb = w / A.nch;
+    const long long a0 = nb * A.npb;
+    const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+    const int kb = __ldg(A.node_ptr + a0), ke = __ldg(A.node_ptr + a1);
+    const int nsl = ke - kb;
+    if (nsl > A.cap_slots || nsl <= 0) {
+        if (nsl > A.cap_slots && A.status) atomicOr(A.status, 2);
+        mbar_arrive_expect_tx(bar, 0);
+        return;
+    }
+    const uint32_t b_rec = (uint32_t)nsl * 16u;
+    const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
+    mbar_arrive_expect_tx(bar, b_rec + 2 * b_slab);
+    bulk_g2s(smem_u32(srec), A.rec + kb, b_rec, bar);
+    bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
+    bulk_g2s(smem_u32(sown), A.own + (size_t)kb * kOwnStride, b_slab, bar);
+}
+
+template <typename T, int V, bool DIFF, bool GM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_reverse_fanp(RevArgs<T> A, long long n_items) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const size_t cap = (size_t)A.cap_slots;
+    const size_t stage_bytes = cap * (16 + 2 * kSlabStride * sizeof(T));
+    // stage q: records, stiffness rows, owner blocks at smem + 16 + q * stage_bytes
+    const uint32_t bar0 = smem_u32(smem);
+    auto srec_of = [&](int q) {
+        return reinterpret_cast<int4*>(smem + 16 + q * stage_bytes);
+    };
+    auto sslab_of = [&](int q) {
+        return reinterpret_cast<T*>(smem + 16 + q * stage_bytes + cap * 16);
+    };
+    auto sown_of = [&](int q) { return sslab_of(q) + cap * kSlabStride; };
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+    }
+    __syncthreads();
+    long long w = blockIdx.x;
+    if (threadIdx.x == 0 && w < n_items) revp_issue<T>(A, w, bar0, srec_of(0), sslab_of(0), sown_of(0));
+    const size_t S = (size_t)A.S;
+    for (int it = 0; w < n_items; w += gridDim.x, ++it) {
+        const int sg = it & 1;
+        const long long wn = w + gridDim.x;
+        if (threadIdx.x == 0 && wn < n_items)
+            revp_issue<T>(A, wn, bar0 + 8 * (sg ^ 1), srec_of(sg ^ 1), sslab_of(sg ^ 1),
+                          sown_of(sg ^ 1));
+        const long long nb = w / A.nch;
+        const int chunk = (int)(w - nb * A.nch);
+        const long long a0 = nb * A.npb;
+        const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+        const long long a = a0 + warp;
+        const bool active = warp < A.npb && a < a1;
+        const size_t col = ((size_t)chunk * 32 + lane) * V;
+        const size_t row = (size_t)a * 3 * S + col;
+        Vec<T, V> ua[3], ca[3];
+        if (active) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ua[d] = ldg<T, V>(A.u + row + d * S);
+                ca[d] = ldg<T, V>(A.x + row + d * S);
+                prefetch_l2(A.uo + row + d * S);
+                prefetch_l2(A.xo + row + d * S);
+            }
+            prefetch_l2(A.invm + (size_t)a * S + col);
+        }
+        if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
+            rev_prefetch<T, GM>(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
+        if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
+            if (lane == 0 && A.status) atomicOr(A.status, 1);
+            return;
+        }
+        if (active) {
+            const int4* srec = srec_of(sg);
+            const T* sslab = sslab_of(sg);
+            const T* sown = sown_of(sg);
+            const int kb = __ldg(A.node_ptr + a0);
+            Vec<T, V> accU[3], accC[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                accU[d] = vzero<T, V>();
+                accC[d] = vzero<T, V>();
+            }
+            const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+            if (k0 < k1) {
+                Vec<T, V> U0[3], U1[3], U2[3], X0[3], X1[3], X2[3], c0, c1, c2;
+                const int4 r0 = srec[k0];
+                load3<T, V>(U0, A.u, r0.y, S, col);
+                load3<T, V>(X0, A.x, r0.y, S, col);
+                load3<T, V>(U1, A.u, r0.z, S, col);
+                load3<T, V>(X1, A.x, r0.z, S, col);
+                c1 = ldg<T, V>(A.coef + (size_t)r0.x * S + col);
+                diff3<T, V, DIFF>(U0, ua);
+                diff3<T, V, DIFF>(X0, ca);
+                int k = k0;
+                while (true) {
+                    rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC,
+                                          U0, X0, U1, X1, c1, U2, X2, c2);
+                    if (k >= k1) break;
+                    rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC,
+                                          U1, X1, U2, X2, c2, U0, X0, c0);
+                    if (k >= k1) break;
+                    rev_phase<T, V, DIFF>(k, k1, srec, sslab, sown, A, S, col, ua, ca, accU, accC,
+                                          U2, X2, U0, X0, c0, U1, X1, c1);
+                    if (k >= k1) break;
+                }
+            }
+            rev_epilogue<T, V, GM>(A, a, S, col, row, ua, ca, accU, accC);
+        }
+        __syncthreads();
+    }
+}
+
 // dJ/dlogE = -c Gamma; dJ/dlogh = -c Gamma - h sum_a alpha_{e,a} G_a / m_a.
 template <typename T>
 __global__ void k_grad_final(long long n_elems, int S, const int32_t* __restrict__ elems,
@@ -641,7 +765,8 @@ __global__ void k_grad_final(long long n_elems, int S, const int32_t* __restrict
 struct RevTuning {
     int vec;      // samples per thread (upper bound)
     int npb;      // nodes (warps) per block of the fan kernel
-    int variant;  // 0: L1-gather kernel; 1: fan-rotation kernel with staged slots
+    int variant;  // 0: L1-gather kernel; 1: fan-rotation kernel with staged slots;
+                  // 2: as 1, persistent, the next item's slots staged under the current
     int minb;     // resident blocks per SM asked of the compiler (fan kernel)
 };
 // Defaults from sweeps on the 256x1024 tube (FP32 128 samples, FP64 64 samples) on B200.
@@ -679,9 +804,47 @@ int launch_rev_fan_m(int minb, unsigned grid, int threads, size_t smem, cudaStre
     }
 }
 
+// The persistent reverse kernel on as many blocks as are resident (at most one per item).
+template <typename Kern, typename T>
+int launch_rev_fanp(Kern kernel, long long n_items, int threads, size_t smem, cudaStream_t st,
+                    const RevArgs<T>& A) {
+    int per_sm = 0;
+    const int rc =
+        fanp_blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem, &per_sm);
+    if (rc) return rc;
+    long long blocks = (long long)per_sm * device_sm_count();
+    if (blocks > n_items) blocks = n_items;
+    kernel<<<(unsigned)blocks, threads, smem, st>>>(A, n_items);
+    CVFES_LAUNCH_CHECK("k_reverse_fanp");
+    return CVFES_OK;
+}
+
+template <typename T, int V, bool DIFF, bool GM>
+int launch_rev_fanp_m(int minb, long long n_items, int threads, size_t smem, cudaStream_t st,
+                      const RevArgs<T>& A) {
+    switch (minb) {
+        case 3:
+            return launch_rev_fanp(k_reverse_fanp<T, V, DIFF, GM, 3>, n_items, threads, smem, st,
+                                   A);
+        case 2:
+            return launch_rev_fanp(k_reverse_fanp<T, V, DIFF, GM, 2>, n_items, threads, smem, st,
+                                   A);
+        default:
+            return launch_rev_fanp(k_reverse_fanp<T, V, DIFF, GM, 1>, n_items, threads, smem, st,
+                                   A);
+    }
+}
+
 template <typename T, int V, bool DIFF>
 int launch_rev_v(const RevTuning& tu, bool fan, bool gmv, unsigned fan_grid, size_t smem,
                  const RowGrid& rg, cudaStream_t st, const RevArgs<T>& A) {
+    if (fan && tu.variant == 2) {
+        const int threads = 32 * tu.npb;
+        const size_t smem2 = 16 + 2 * (smem - 16);
+        return gmv ? launch_rev_fanp_m<T, V, DIFF, true>(tu.minb, fan_grid, threads, smem2, st, A)
+                   : launch_rev_fanp_m<T, V, DIFF, false>(tu.minb, fan_grid, threads, smem2, st,
+                                                          A);
+    }
     if (fan) {
         const int threads = 32 * tu.npb;
         return gmv ? launch_rev_fan_m<T, V, DIFF, true>(tu.minb, fan_grid, threads, smem, st, A)
@@ -742,8 +905,8 @@ int launch_reverse_step(const cvfes_adjoint_desc* d, const T* u, T* uo, const T*
     A.cap_slots = 0;
     const long long cap = (long long)tu.npb * m->max_degree;
     const size_t smem = 16 + (size_t)cap * (16 + (kSlabStride + kOwnStride) * sizeof(T));
-    const bool fan = tu.variant == 1 && m->max_degree > 0 && (A.S / V) % 32 == 0 &&
-                     smem <= kRevMaxStage && tu.npb >= 1 && tu.npb <= 8;
+    const bool fan = (tu.variant == 1 || tu.variant == 2) && m->max_degree > 0 &&
+                     (A.S / V) % 32 == 0 && smem <= kRevMaxStage && tu.npb >= 1 && tu.npb <= 8;
     unsigned fan_grid = 0;
     if (fan) {
         A.npb = tu.npb;
@@ -951,8 +1114,8 @@ using namespace cvfes;
 extern "C" int cvfes_set_adjoint_tuning(int32_t precision, int32_t vec, int32_t npb,
                                         int32_t variant, int32_t minb) {
     if ((precision != 32 && precision != 64) || (vec != 1 && vec != 2 && vec != 4) ||
-        (precision == 64 && vec == 4) || npb < 1 || npb > 8 || variant < 0 || variant > 1 ||
-        minb < 1 || minb > 4)
+        (precision == 64 && vec == 4) || npb < 1 || npb > 8 || variant < 0 || variant > 2 ||
+        minb < 1 || minb > 4 || (variant == 2 && minb > 3))
         return fail(CVFES_ERR_ARG, "cvfes_set_adjoint_tuning: bad argument");
     RevTuning& t = precision == 32 ? g_rev32 : g_rev64;
     t = RevTuning{vec, npb, variant, minb};

@@ -1151,6 +1151,8 @@ int launch_pipe(const StepArgs<T>& A, long long max_deg, int warps, int stages, 
 // Resident blocks per SM of a persistent kernel at this block size and shared memory,
 // with the shared-memory attribute set when it needs more than 48 KB; looked up once
 // per (kernel, device, block, shared memory) and kept, since every step launches it.
+int device_sm_count() { return sm_count(); }
+
 int fanp_blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm) {
     struct Entry {
         const void* k;

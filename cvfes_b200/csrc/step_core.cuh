@@ -605,6 +605,11 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+// Resident blocks per SM of a persistent kernel (solid_step.cu; cached per kernel,
+// device, block size and shared memory) and the device's SM count.
+int fanp_blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm);
+int device_sm_count();
+
 // TMA-tiled step (solid_tile.cu): returns 1 without launching when the mesh has no
 // tiling or the shape does not fit the tiled kernel.
 template <typename T>

@@ -539,8 +539,9 @@ typedef struct cvfes_adjoint_desc {
 
 /* Reverse-step kernel choice per precision: samples per thread (1|2|4, FP64 1|2),
  * nodes per block (1..8), variant (0: L1 gather, 1: fan rotation with TMA-staged
- * slot rows, needing S/vec a multiple of 32), minimum blocks per SM (1..4, a register
- * cap).  Every choice gives bitwise the same results. */
+ * slot rows, needing S/vec a multiple of 32; 2: as 1, persistent, each block staging
+ * its next work item's slot rows while it runs the current one, minb 1..3), minimum
+ * blocks per SM (1..4, a register cap).  Every choice gives bitwise the same results. */
 int cvfes_set_adjoint_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t variant,
                              int32_t minb);
 int cvfes_get_adjoint_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t* variant,

@@ -136,14 +136,17 @@ def test_problem_rejects_bad_observation_nodes(lib, cuda):
 
 
 REV_VARIANTS = {
-    32: [(4, 8, 0, 1), (2, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 2), (4, 2, 1, 1), (2, 4, 1, 2)],
-    64: [(2, 8, 0, 1), (1, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 1), (2, 4, 1, 2)],
+    32: [(4, 8, 0, 1), (2, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 2), (4, 2, 1, 1), (2, 4, 1, 2),
+         (2, 2, 2, 2), (4, 2, 2, 1), (2, 4, 2, 2)],
+    64: [(2, 8, 0, 1), (1, 8, 0, 1), (1, 2, 1, 2), (2, 2, 1, 1), (2, 4, 1, 2), (2, 2, 2, 1),
+         (1, 2, 2, 2)],
 }
 
 
 @pytest.mark.parametrize("precision", [32, 64])
 def test_reverse_kernel_variants_are_bitwise_identical(lib, cuda, precision):
-    """L1-gather and fan-rotation reverse kernels, every tile shape: same bits."""
+    """L1-gather, fan-rotation and persistent fan reverse kernels, every tile shape:
+    same bits."""
     from cvfes_b200 import _lib
     case = dataclasses.replace(SMALL, n_samples=128 if precision == 32 else 64)
     p, logE, logh, _ = adjoint_setup(case, precision=precision, device=cuda, grad_logh=True)
