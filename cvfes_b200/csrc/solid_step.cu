@@ -420,8 +420,9 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
             prefetch_l2(A.invm + (size_t)a * S + col);
             node_load<T>(A, a, p, f);
         }
-        if (A.pf_dist > 0 && chunk == 0 && nb % A.pf_group == 0 && warp == A.npb - 1)
-            fan_prefetch(A, a0 + A.pf_dist, A.npb * A.pf_group, lane);
+        // No L2 prefetch ahead here: the prefetching warp's dependent slot-record loads
+        // hold its whole block at the item barrier (measured 2.466 -> 3.579 ms/step on the
+        // 256x1024 tube with it; node rows alone 3.06 ms).
         if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
             if (lane == 0 && A.status) atomicOr(A.status, 1);
             return;

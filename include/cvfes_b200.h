@@ -120,7 +120,7 @@ int cvfes_set_step_tuning(int32_t precision, int32_t vec, int32_t npb, int32_t s
 int cvfes_get_step_tuning(int32_t precision, int32_t* vec, int32_t* npb, int32_t* staged,
                           int32_t* minb);
 
-/* L2 prefetch of the fan step kernels (staged 3, 6, 8) and the fan reverse step:
+/* L2 prefetch of the fan step kernels (staged 3 and 8) and the fan reverse step:
  * each node block's first sample chunk prefetches into L2, by bulk prefetches, rows
  * that the nodes `distance` ahead of it will read.
  *   distance: in nodes; -1 (default) = the mesh's bandwidth + 128 (off when the
