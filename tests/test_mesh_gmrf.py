@@ -146,3 +146,89 @@ def test_gmrf_matches_oracle_restatement(lib):
     z = g.sample(12, seed=5)
     zo = o.sample(12, seed=5, columns=[0, 7, 11])
     assert np.max(np.abs(z[:, [0, 7, 11]] - zo)) < 1e-10
+
+
+def _reference_module(filename):
+    """Import a module of the reference checkout (CVFES_REFERENCE, else `reference` beside
+    this repository) with stubs for the modules it imports at load time but the tested
+    functions never use (mesh, mpi4py, parmetis).  None when the checkout is absent."""
+    import importlib.util
+    import os
+    import sys
+    import types
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    ref = os.environ.get("CVFES_REFERENCE") or os.path.join(root, "reference")
+    path = os.path.join(ref, filename)
+    if not os.path.exists(path):
+        return None
+    stubs = {"mesh": types.ModuleType("mesh"), "mpi4py": types.ModuleType("mpi4py"),
+             "parmetis": types.ModuleType("parmetis")}
+    stubs["mpi4py"].MPI = None
+    stubs["parmetis"].PyParMETIS_V3_PartMeshKway = None
+    saved = {k: sys.modules.get(k) for k in stubs}
+    sys.modules.update(stubs)
+    try:
+        spec = importlib.util.spec_from_file_location("ref_" + filename[:-3], path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+    return mod
+
+
+class _RaggedNumpy:
+    """numpy for code written for NumPy 1.x: np.array of ragged lists gives an object
+    array (NumPy 2 raises instead); everything else is numpy itself."""
+
+    def __getattr__(self, name):
+        return getattr(np, name)
+
+    @staticmethod
+    def array(x, *args, **kw):
+        try:
+            return np.array(x, *args, **kw)
+        except ValueError:
+            out = np.empty(len(x), dtype=object)
+            for i, item in enumerate(x):
+                out[i] = item
+            return out
+
+
+def test_greedy_colouring_matches_reference_module(lib, tmp_path, monkeypatch):
+    """cvfes_mesh_color_greedy against the reference's own MeshColoring
+    (meshColoring.py:7-63), run here on the same mesh: identical colours."""
+    from cvfes_b200.plan import color_greedy
+    mod = _reference_module("meshColoring.py")
+    if mod is None:
+        pytest.skip("reference checkout not found")
+    mod.np = _RaggedNumpy()
+    nodes, elems, inl, outl = tube_mesh(TubeGeometry(16, 12, 3.0))
+    lcl, lel, lb, nb = special_assignment(elems, len(nodes), np.concatenate([inl, outl]))
+    stub = type("M", (), dict(lclNNodes=len(nodes), nElements=len(elems), lclElmNodeIds=lel))()
+    monkeypatch.chdir(tmp_path)
+    assert mod.MeshColoring("colors", stub) == 0
+    ours, n = color_greedy(lel, len(nodes))
+    assert np.array_equal(np.asarray(stub.elmColors, dtype=np.int64), ours.astype(np.int64))
+    assert n == len(stub.colorGroups)
+
+
+def test_special_assignment_matches_reference_module():
+    """mesh.special_assignment against the reference's SolidMeshPartition.SpecialAssignment
+    (meshPartition.py:240-254), run here: identical numbering."""
+    mod = _reference_module("meshPartition.py")
+    if mod is None:
+        pytest.skip("reference checkout not found")
+    mod.np = _RaggedNumpy()
+    if not hasattr(np, "in1d"):
+        mod.np.in1d = np.isin
+    nodes, elems, inl, outl = tube_mesh(TubeGeometry(16, 12, 3.0))
+    bdy = np.concatenate([inl, outl])
+    stub = type("M", (), dict(nNodes=len(nodes), boundary=bdy, elementNodeIds=elems))()
+    mod.SolidMeshPartition.SpecialAssignment(None, stub)
+    lcl, lel, lb, nb = special_assignment(elems, len(nodes), bdy)
+    assert np.array_equal(stub.lclNodeIds, lcl) and np.array_equal(stub.lclElmNodeIds, lel)
+    assert np.array_equal(stub.lclBoundary, lb) and stub.lclNSpecialHead == nb
