@@ -769,9 +769,12 @@ struct RevTuning {
                   // 2: as 1, persistent, the next item's slots staged under the current
     int minb;     // resident blocks per SM asked of the compiler (fan kernel)
 };
-// Defaults from sweeps on the 256x1024 tube (FP32 128 samples, FP64 64 samples) on B200.
+// Defaults from sweeps on B200: FP32 on the 256x1024 tube with 128 samples and the
+// stenosed 512x2048 tube (reverse 6.25 s per 1000 steps; the persistent variant 7.89 s);
+// FP64 on the 64x128 tube with 64 samples (reverse pass of 500 steps: vec 1 with 4 nodes
+// per block 29.6 ms, vec 2 with 2 nodes 30.6 ms, persistent 30.2 ms).
 static RevTuning g_rev32 = {2, 2, 1, 2};
-static RevTuning g_rev64 = {2, 2, 1, 1};
+static RevTuning g_rev64 = {1, 4, 1, 2};
 template <typename T>
 RevTuning& rev_tuning() {
     return sizeof(T) == 4 ? g_rev32 : g_rev64;

@@ -1054,10 +1054,10 @@ struct StepTuning {
     int minb;  // minimum resident blocks per SM asked of the compiler (register cap)
 };
 // Defaults from sweeps on the 256x1024 tube with 512 samples (B200), ms/step:
-// FP32 (velocity-state form): persistent fan 2.489, fan 2.618, fan with loads two
-// elements ahead 2.637, fan with 4 nodes per block 2.591; FP64: fan 5.750, persistent
-// fan 6.088, two ahead 5.981.  2 nodes per block, 2 blocks per SM worth of registers.
-static StepTuning g_tune32 = {4, 2, 6, 2};
+// FP32 (velocity-state form): persistent fan 2.441 (4 nodes per block), 2.445 (2), 2.562
+// (3), fan 2.606 (2), 2.598 (4), fan with loads two elements ahead 2.637; FP64: fan 5.750,
+// persistent fan 6.088, two ahead 5.981.  2 blocks per SM worth of registers.
+static StepTuning g_tune32 = {4, 4, 6, 2};
 static StepTuning g_tune64 = {2, 2, 3, 2};
 // L2 prefetch of the fan kernels: distance in nodes (-1: the mesh's bandwidth + 128;
 // 0: off) and parts (bit 0 node rows, bit 1 element coefficient rows; -1: automatic).

@@ -16,7 +16,8 @@ Here the GPU advances the WHOLE ensemble of each workload with the default kerne
 (FP64 state, and the default FP32 state form; the batch tubes through the batched
 kernels) and the chunk's samples are compared:
 relative L2 against the truth over the fixture's 2048 nodes and the per-sample sum over
-all nodes of u^2: FP64 <= 1e-12 (2e-12 for the sum), FP32 <= 1e-5 (2e-5); against the
+all nodes of u^2: FP64 <= 1e-12 (2e-12 for the sum) or, where the reference's own FP64
+run is further than that from the truth, no further than it; FP32 <= 1e-5 (2e-5); against the
 reference's FP64 run, within that run's own distance from the truth plus the gate; and
 for FP64 the sum of the last increment squared, <= 1e-9 of the reference's (the
 increment is small against u, so its relative error is larger).
@@ -117,7 +118,9 @@ def test_full_run_against_reference(lib, cuda, name, precision):
           f"FP64 {err_ref:.3e} (reference FP64 vs long double {ref_err:.3e}), sum u^2 "
           f"{e_u2:.3e}, sum du^2 vs reference {e_du2:.3e}")
     assert np.all(nrm[:, 3] == 0)
-    assert err <= TOL[precision]
+    # FP64 can fall short of 1e-12 over a long run on a badly conditioned tube; the bar is
+    # then the reference's own FP64 error against the truth (tube 58: 7.0e-12)
+    assert err <= max(TOL[precision], ref_err)
     assert e_u2 <= 2 * TOL[precision]
     # against the reference's own FP64 run: within its distance from the truth plus the gate
     assert err_ref <= ref_err + TOL[precision]
