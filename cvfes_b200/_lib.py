@@ -123,9 +123,9 @@ SIGNATURES = {
     "cvfes_solid_step_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, P, D, D, P]),
     "cvfes_solid_step_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, P, D, D, P]),
     "cvfes_solid_step_norms_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, P, D, D, P, P,
-                                             I32, P]),
+                                             P, I32, P]),
     "cvfes_solid_step_norms_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, P, D, D, P, P,
-                                             I32, P]),
+                                             P, I32, P]),
     "cvfes_solid_advance_f64": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, D, P, P, P]),
     "cvfes_solid_advance_f32": (C.c_int, [DESC, P, P, P, P, P, P, P, I64, D, D, P, P, P]),
     "cvfes_solid_init_f64": (C.c_int, [DESC, P, P, P, P, P, P, D, D, D, P]),

@@ -1609,7 +1609,8 @@ template <typename T>
 int launch_step_norms(const cvfes_solid_mesh* m, const T* coef, const T* invm, const T* u,
                       const T* up, T* un, const double* p_sched, const long long* clock,
                       long long j, double pressure, const T* trac, double dt, double damp,
-                      double* work, double* out, int check_finite, cudaStream_t st) {
+                      double* work, double* out, double* out_host, int check_finite,
+                      cudaStream_t st) {
     int rc = check_mesh(m, "cvfes_solid_step_norms");
     if (rc) return rc;
     if (!work || !out) return fail(CVFES_ERR_ARG, "cvfes_solid_step_norms: null work or out");
@@ -1620,19 +1621,37 @@ int launch_step_norms(const cvfes_solid_mesh* m, const T* coef, const T* invm, c
                         work, &rows, max_rows);
     if (rc) return rc;
     const bool vel = m->state_form == 1;
-    if (rows == 0)  // no fused kernel for this shape: the separate pass over the new state
-        return launch_norms<T>(N, S, un, vel ? up : u, invm, work, out, check_finite, st, vel);
-    double* total = work + (size_t)rows * S * 4;
-    CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
-    k_norms_final<<<final_grid(S), kFinalPairs * kFinalGroups, 0, st>>>(rows, (int)S, work, out, total);
-    CVFES_LAUNCH_CHECK("k_norms_final");
-    if (check_finite) {
-        double h = 0.0;
-        CVFES_CUDA_TRY(cudaMemcpyAsync(&h, total, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CVFES_CUDA_TRY(cudaStreamSynchronize(st));
-        if (h != 0.0)
-            return fail(CVFES_ERR_NONFINITE, "watchdog: %.0f non-finite state values", h);
+    double* total = nullptr;
+    if (rows == 0) {  // no fused kernel for this shape: the separate pass over the new state
+        rc = launch_norms<T>(N, S, un, vel ? up : u, invm, work, out, out_host ? 0 : check_finite,
+                             st, vel);
+        if (rc) return rc;
+        total = work + (size_t)norm_chunks(N) * S * 4;
+    } else {
+        total = work + (size_t)rows * S * 4;
+        CVFES_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(double), st));
+        k_norms_final<<<final_grid(S), kFinalPairs * kFinalGroups, 0, st>>>(rows, (int)S, work,
+                                                                            out, total);
+        CVFES_LAUNCH_CHECK("k_norms_final");
     }
+    if (!out_host && !check_finite) return CVFES_OK;
+    // one synchronisation for everything the host reads: the norms (out_host), the
+    // non-finite total and the status word of the bounded waits (read and cleared)
+    double h = 0.0;
+    int32_t stat = 0;
+    if (out_host)
+        CVFES_CUDA_TRY(cudaMemcpyAsync(out_host, out, (size_t)S * 4 * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
+    CVFES_CUDA_TRY(cudaMemcpyAsync(&h, total, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (out_host && m->status) {
+        CVFES_CUDA_TRY(cudaMemcpyAsync(&stat, m->status, sizeof(stat), cudaMemcpyDeviceToHost, st));
+        CVFES_CUDA_TRY(cudaMemsetAsync(m->status, 0, sizeof(int32_t), st));
+    }
+    CVFES_CUDA_TRY(cudaStreamSynchronize(st));
+    if (stat & 1) return fail(CVFES_ERR_TIMEOUT, "a bounded device wait gave up (status %d)", stat);
+    if (stat) return fail(CVFES_ERR_ARG, "device status %d: slot stage overflow", stat);
+    if (check_finite && h != 0.0)
+        return fail(CVFES_ERR_NONFINITE, "watchdog: %.0f non-finite state values", h);
     return CVFES_OK;
 }
 
@@ -1642,20 +1661,23 @@ extern "C" int cvfes_solid_step_norms_f64(const cvfes_solid_mesh* mesh, const do
                                           const double* p_sched, const int64_t* clock, int64_t j,
                                           double pressure, const double* trac, double dt,
                                           double damp, double* work, double* out,
-                                          int32_t check_finite, void* stream) {
+                                          double* out_host, int32_t check_finite, void* stream) {
     return launch_step_norms<double>(mesh, coef, invm, u, u_prev, u_next, p_sched,
                                      reinterpret_cast<const long long*>(clock), j, pressure, trac,
-                                     dt, damp, work, out, check_finite, (cudaStream_t)stream);
+                                     dt, damp, work, out, out_host, check_finite,
+                                     (cudaStream_t)stream);
 }
 extern "C" int cvfes_solid_step_norms_f32(const cvfes_solid_mesh* mesh, const float* coef,
                                           const float* invm, const float* u, const float* u_prev,
                                           float* u_next, const double* p_sched,
                                           const int64_t* clock, int64_t j, double pressure,
                                           const float* trac, double dt, double damp, double* work,
-                                          double* out, int32_t check_finite, void* stream) {
+                                          double* out, double* out_host,
+                                          int32_t check_finite, void* stream) {
     return launch_step_norms<float>(mesh, coef, invm, u, u_prev, u_next, p_sched,
                                     reinterpret_cast<const long long*>(clock), j, pressure, trac,
-                                    dt, damp, work, out, check_finite, (cudaStream_t)stream);
+                                    dt, damp, work, out, out_host, check_finite,
+                                    (cudaStream_t)stream);
 }
 
 extern "C" int cvfes_solid_advance_f64(const cvfes_solid_mesh* mesh, const double* coef,

@@ -226,7 +226,8 @@ class GPUSolidSolver(PhysicsSolver):
             self._graphs = {}
             self._p_buf = None
             self._norm_out = None
-            self._norms_step = -1  # step_count at which _norm_out was fused into a step
+            self._norm_host = None  # pinned copy of the fused norms, read with the step
+            self._norms_step = -1  # step_count at which the norms were fused into a step
             self.step_count = 0
             self.geo_counter = 0
             self.geo_live = False
@@ -323,8 +324,13 @@ class GPUSolidSolver(PhysicsSolver):
                 if self._norm_out is None:
                     self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
                                                  device=self.device)
+                if self._norm_host is None:
+                    self._norm_host = torch.empty((self.nSmp, 4), dtype=torch.float64,
+                                                  pin_memory=True)
+                # the call returns with the norms in _norm_host and the status word of
+                # the bounded waits read and cleared (one stream synchronisation)
                 call(fn.replace("step_", "step_norms_"), *args, ptr(self.norm_work),
-                     ptr(self._norm_out), 0, self._stream())
+                     ptr(self._norm_out), ptr(self._norm_host), 0, self._stream())
             else:
                 call(fn, *args, self._stream())
         self._rotate()
@@ -468,26 +474,32 @@ class GPUSolidSolver(PhysicsSolver):
 
         ``out``: an (S, 4) FP64 host tensor (pinned, for an asynchronous copy) that
         receives the result; the call returns once it has arrived."""
-        if self._norm_out is None:
-            self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
-                                         device=self.device)
-        dev_out = self._norm_out
-        fresh = self._norms_step == self.step_count  # fused into the last step
-        fn = "cvfes_solid_norms_f64" if self.precision == 64 else "cvfes_solid_norms_f32"
-        if self.state_form == "velocity":
-            fn = fn.replace("norms_", "norms_vel_")
         chk = self.watchdog if check_finite is None else check_finite
-        with torch.cuda.device(self.device):
-            if not fresh:
+        fresh = self._norms_step == self.step_count  # fused into the last step
+        if fresh:  # already on the host, status checked by the step call
+            if out is None:
+                res = self._norm_host.clone()
+            else:
+                out.copy_(self._norm_host)
+                res = out
+        else:
+            if self._norm_out is None:
+                self._norm_out = torch.empty((self.nSmp, 4), dtype=torch.float64,
+                                             device=self.device)
+            dev_out = self._norm_out
+            fn = "cvfes_solid_norms_f64" if self.precision == 64 else "cvfes_solid_norms_f32"
+            if self.state_form == "velocity":
+                fn = fn.replace("norms_", "norms_vel_")
+            with torch.cuda.device(self.device):
                 call(fn, self.lclNNodes, self.nSmp, ptr(self.bufs[self.cur]),
                      ptr(self.bufs[self.prev]), ptr(self.plan.invm(self.precision)),
                      ptr(self.norm_work), ptr(dev_out), int(bool(chk)), self._stream())
-            if out is None:
-                res = dev_out.cpu()
-            else:
-                out.copy_(dev_out, non_blocking=True)
-                res = out
-            self.plan.check_status()
+                if out is None:
+                    res = dev_out.cpu()
+                else:
+                    out.copy_(dev_out, non_blocking=True)
+                    res = out
+                self.plan.check_status()
         res = res.numpy()
         if fresh and chk and np.any(res[:, 3] != 0):
             raise _lib.NonFiniteError(_lib.CVFES_ERR_NONFINITE,

@@ -292,20 +292,23 @@ int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef, const 
  * writes the state, so the state is not read a second time; shapes without it (S / vec
  * not a multiple of 32, no max_degree) run the step and the separate norms pass.
  * work: cvfes_norms_work_size(N, S) doubles.  check_finite: as cvfes_solid_norms_*.
+ * out_host (NULL, or S*4 doubles of pinned host memory): when given, the call also copies
+ * out to out_host, reads and clears mesh->status (CVFES_ERR_TIMEOUT if a bounded wait
+ * gave up) and returns after one stream synchronisation with the norms on the host.
  * Replaces the reference's per-step host round trip of the state
  * (physicsSolverSDampGPUs.py:363-390) with one small read-back of per-sample sums.   */
 int cvfes_solid_step_norms_f64(const cvfes_solid_mesh* mesh, const double* coef,
                                const double* invm, const double* u, const double* u_prev,
                                double* u_next, const double* p_sched, const int64_t* clock,
                                int64_t j, double pressure, const double* trac, double dt,
-                               double damp, double* work, double* out, int32_t check_finite,
-                               void* stream);
+                               double damp, double* work, double* out, double* out_host,
+                               int32_t check_finite, void* stream);
 int cvfes_solid_step_norms_f32(const cvfes_solid_mesh* mesh, const float* coef,
                                const float* invm, const float* u, const float* u_prev,
                                float* u_next, const double* p_sched, const int64_t* clock,
                                int64_t j, double pressure, const float* trac, double dt,
-                               double damp, double* work, double* out, int32_t check_finite,
-                               void* stream);
+                               double damp, double* work, double* out, double* out_host,
+                               int32_t check_finite, void* stream);
 
 /* n_steps steps with the buffer rotation (u_next, u, u_prev) <- (u_prev, u_next, u)
  * of physicsSolverSDampGPUs.py:398-399.  bufs[0] = u_n, bufs[1] = u_{n-1},
