@@ -643,7 +643,7 @@ def main():
         raise SystemExit("--chunk must be a multiple of 6")
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload in ("batched64", "adjoint64", "stenosed512x2048"):
+    if args.workload in ("batched64", "adjoint64", "stenosed512x2048", "stenosed256x512"):
         return run_workload(args)
     return run_gpu(args)
 

@@ -9,6 +9,7 @@ tube sizes, material law and load follow the workload definitions:
                  S in {16..256}, per-tube CFL dt, 1000 steps
 ``adjoint64``    tube64x128 mesh, 64 samples, 500 steps, 512 observation nodes
 ``stenosed512x2048`` stenosed tube L=5 cm, 512 x 2048 nodes, 128 samples, 1000 steps
+``stenosed256x512``  the same tube at 256 x 512 nodes, 128 samples, 100 steps (profiles)
 
 Material: ``E = 7e6*exp(0.2 z)``, ``h = 0.04*exp(0.1 z')`` with z, z' independent
 per-element GMRF samples (:mod:`cvfes_b200.gmrf`); nu = 0.49, rho = 1,
@@ -77,6 +78,12 @@ CASES = {
                             mass_lumping="rowsum"),
     "adjoint64": TubeCase("adjoint64", 64, 128, 3.0, n_samples=64, dt=2e-6, n_steps=500,
                           extra=dict(n_obs=512, obs_every=10, ckpt_every=50)),
+    # the stenosed adjoint at half the resolution each way and a tenth of the steps, for
+    # kernel profiles of the reverse step: 0.2 GB per state (1.6x L2), 2 checkpoint pairs
+    "stenosed256x512": TubeCase("stenosed256x512", 256, 512, 5.0, stenosed=True,
+                                n_samples=128, dt=None, n_steps=100,
+                                extra=dict(n_obs=1024, obs_every=10, ckpt_every=50,
+                                           grad_logh=True)),
     "stenosed512x2048": TubeCase("stenosed512x2048", 512, 2048, 5.0, stenosed=True,
                                  n_samples=128, dt=None, n_steps=1000,
                                  extra=dict(n_obs=4096, obs_every=10, ckpt_every=100,

@@ -962,28 +962,30 @@ __global__ void k_norms_partial(long long n_nodes, int S, long long npc, const T
     const int s = blockIdx.y * kNormThreads + threadIdx.x;
     if (s >= S) return;
     const long long a0 = chunk * npc, a1 = (a0 + npc < n_nodes) ? a0 + npc : n_nodes;
-    double su = 0.0, sv = 0.0, sm = 0.0, nf = 0.0;
+    double su = 0.0, sv = 0.0, sm = 0.0;
+    long long nf = 0;
     for (long long a = a0; a < a1; ++a) {
-        const double im = (double)invm[(size_t)a * S + s];
-        const double m = im != 0.0 ? 1.0 / im : 0.0;
-        double dv2 = 0.0;
+        // the node terms in the state's type, in the fused step's order (norms_add)
+        const T im = invm[(size_t)a * S + s];
+        T su_a = T(0), dv2 = T(0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const size_t o = ((size_t)a * 3 + d) * S + s;
-            const double x = (double)u[o], y = (double)up[o];
-            if (!isfinite(x)) nf += 1.0;
-            su += x * x;
-            const double dv = VEL ? y : x - y;
-            dv2 += dv * dv;
+            const T x = u[o], y = up[o];
+            if (!isfinite(x)) ++nf;
+            su_a = fma(x, x, su_a);
+            const T dv = VEL ? y : x - y;
+            dv2 = fma(dv, dv, dv2);
         }
-        sv += dv2;
-        sm += m * dv2;
+        su += (double)su_a;
+        sv += (double)dv2;
+        sm += (double)(norm_mass(im) * dv2);
     }
     double* w = work + ((size_t)chunk * S + s) * 4;
     w[0] = su;
     w[1] = sv;
     w[2] = sm;
-    w[3] = nf;
+    w[3] = (double)nf;
 }
 
 // Sums of the partial rows per (sample, quantity): a block owns kFinalPairs consecutive

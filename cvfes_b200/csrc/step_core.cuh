@@ -72,19 +72,28 @@ __device__ __forceinline__ T row_eta(const StepArgs<T>& A, T im) {
     return A.damp_per_dof ? A.eta * im : A.eta;
 }
 
+// Norm terms of one node (sum of squares of its three new values, of its three
+// increments, and the count of non-finite values) are formed in the state's type and
+// only the node sums are taken to FP64: with the FP32 state each node term carries
+// three FP32 roundings (five for the mass-weighted one: <= 3e-7 relative, all terms
+// positive, so the sum over nodes keeps that bound), and the FP64 sums
+// over nodes need three conversions per node instead of seven (a conversion to FP64
+// runs at a quarter of the FP64 rate; per value they cost a tenth of the step).  The
+// separate norms pass forms the same node terms in the same order.
+__device__ __forceinline__ float norm_mass(float im) { return im != 0.f ? __frcp_rn(im) : 0.f; }
+__device__ __forceinline__ double norm_mass(double im) { return im != 0.0 ? 1.0 / im : 0.0; }
+
 // Per-lane accumulator of the fused norms: quantity q of sample i of the lane's vector
 // at nacc[(q * V + i) * 32] (lanes innermost: no shared-memory bank conflicts).
 template <typename T, int V>
-__device__ __forceinline__ void norms_add(double* nacc, const Vec<T, V>& im, const double (&su)[V],
-                                          const double (&sv)[V], const double (&nf)[V]) {
+__device__ __forceinline__ void norms_add(double* nacc, const Vec<T, V>& im, const T (&su)[V],
+                                          const T (&sv)[V], const int (&nf)[V]) {
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-        const double x = (double)im.v[i];
-        const double m = x != 0.0 ? 1.0 / x : 0.0;
-        nacc[(0 * V + i) * 32] += su[i];
-        nacc[(1 * V + i) * 32] += sv[i];
-        nacc[(2 * V + i) * 32] += m * sv[i];
-        nacc[(3 * V + i) * 32] += nf[i];
+        nacc[(0 * V + i) * 32] += (double)su[i];
+        nacc[(1 * V + i) * 32] += (double)sv[i];
+        nacc[(2 * V + i) * 32] += (double)(norm_mass(im.v[i]) * sv[i]);
+        if (nf[i]) nacc[(3 * V + i) * 32] += (double)nf[i];
     }
 }
 
@@ -347,9 +356,13 @@ __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size
                                             double* nacc = nullptr, long long a = 0,
                                             size_t col = 0) {
     const Vec<T, V> cl = vfill<T, V>(A.clamp);
-    double su[V], sv[V], nf[V];
+    T su[V], sv[V];
+    int nf[V];
 #pragma unroll
-    for (int i = 0; i < V; ++i) su[i] = sv[i] = nf[i] = 0.0;
+    for (int i = 0; i < V; ++i) {
+        su[i] = sv[i] = T(0);
+        nf[i] = 0;
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (A.vel || nacc) {
@@ -358,9 +371,9 @@ __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size
             if (nacc) {
 #pragma unroll
                 for (int i = 0; i < V; ++i) {
-                    su[i] += (double)cl.v[i] * (double)cl.v[i];
-                    sv[i] += (double)dv.v[i] * (double)dv.v[i];
-                    nf[i] += isfinite(cl.v[i]) ? 0.0 : 1.0;
+                    su[i] = fma(cl.v[i], cl.v[i], su[i]);
+                    sv[i] = fma(dv.v[i], dv.v[i], sv[i]);
+                    nf[i] += isfinite(cl.v[i]) ? 0 : 1;
                 }
             }
         }
@@ -371,16 +384,20 @@ __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size
 
 // As step_update, reading the row's u_{n-1} (or v_n) and inverse mass here.
 // With nacc (fused norms) the row's contributions to the per-sample sums of u_{n+1}^2,
-// du^2 (v_{n+1}^2, or (u_{n+1} - u_n)^2 in FP64) and m du^2 are added there.
+// du^2 (v_{n+1}^2, or u_{n+1} - u_n) and m du^2 are added there (node terms as norms_add).
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
                                               const Vec<T, V> (&acc)[3], const T (&f)[3],
                                               double* nacc = nullptr) {
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
-    double su[V], sv[V], nf[V];
+    T su[V], sv[V];
+    int nf[V];
 #pragma unroll
-    for (int i = 0; i < V; ++i) su[i] = sv[i] = nf[i] = 0.0;
+    for (int i = 0; i < V; ++i) {
+        su[i] = sv[i] = T(0);
+        nf[i] = 0;
+    }
     if (A.vel) {
         // velocity-state form: v_{n+1} = v_n (1 - eta) + w (p f - K u_n), u_{n+1} = u_n + v_{n+1};
         // a row without mass (u_{n+1} = 0) keeps v_{n+1} = -u_n, the exact increment.
@@ -397,9 +414,9 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
                 o.v[i] = live ? ua[d].v[i] + v : T(0);
                 vn.v[i] = live ? v : -ua[d].v[i];
                 if (nacc) {
-                    su[i] += (double)o.v[i] * (double)o.v[i];
-                    sv[i] += (double)vn.v[i] * (double)vn.v[i];
-                    nf[i] += isfinite(o.v[i]) ? 0.0 : 1.0;
+                    su[i] = fma(o.v[i], o.v[i], su[i]);
+                    sv[i] = fma(vn.v[i], vn.v[i], sv[i]);
+                    nf[i] += isfinite(o.v[i]) ? 0 : 1;
                 }
             }
             stcs<T, V>(A.un + row + d * S, o);
@@ -420,10 +437,10 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
             const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
             if (nacc) {
-                const double du = (double)o.v[i] - (double)ua[d].v[i];
-                su[i] += (double)o.v[i] * (double)o.v[i];
-                sv[i] += du * du;
-                nf[i] += isfinite(o.v[i]) ? 0.0 : 1.0;
+                const T du = o.v[i] - ua[d].v[i];
+                su[i] = fma(o.v[i], o.v[i], su[i]);
+                sv[i] = fma(du, du, sv[i]);
+                nf[i] += isfinite(o.v[i]) ? 0 : 1;
             }
         }
         stcs<T, V>(A.un + row + d * S, o);

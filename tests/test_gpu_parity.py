@@ -196,6 +196,34 @@ def test_norms_and_watchdog(lib, cuda):
     assert s.Norms(check_finite=False)[2, 3] == 1
 
 
+@pytest.mark.parametrize("state", ["velocity", "previous"])
+@pytest.mark.parametrize("norms_every", [0, 1])
+def test_fp32_norms_against_fp64_sums(lib, cuda, state, norms_every):
+    """FP32 state, separate pass and fused into the step: the norms against FP64 sums of
+    the same FP32 values.  Each node's three-value term is formed in FP32 (three
+    roundings; five for the mass-weighted term), so the bound is 2e-7 (3e-7)."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(64)
+    s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 64, 32, chunk=12, state=state,
+                                              norms_every=norms_every))
+    pres = case.pressures(150)
+    for n in range(150):
+        s.pressure = float(pres[n])
+        s.Solve(None, case.dt)
+    nrm = s.Norms()
+    assert s._norms_step == (s.step_count if norms_every else -1)
+    u = s.bufs[s.cur].double().cpu().numpy()
+    other = s.bufs[s.prev].double().cpu().numpy()
+    du = other if state == "velocity" else u - other
+    im = s.plan.invm(32).double().cpu().numpy()
+    m = np.repeat(np.where(im != 0, 1.0 / np.where(im != 0, im, 1.0), 0.0), 3, axis=0)
+    np.testing.assert_allclose(nrm[:, 0], (u ** 2).sum(0), rtol=2e-7, atol=0)
+    np.testing.assert_allclose(nrm[:, 1], (du ** 2).sum(0), rtol=2e-7, atol=0)
+    np.testing.assert_allclose(nrm[:, 2], (m * du ** 2).sum(0), rtol=3e-7, atol=0)
+    assert np.all(nrm[:, 3] == 0)
+
+
 def test_invalid_arguments_are_rejected(lib, cuda):
     mesh = c0_mesh(4)
     s = GPUSolidSolver(LocalComm(), mesh, Cfg(2e-6, 4, 64))
