@@ -368,10 +368,16 @@ __device__ __forceinline__ void fanp_issue(const StepArgs<T>& A, long long w, ui
 }
 
 // With A.norm_part (fused norms) the grid is a multiple of nch, so block b always has
-// sample chunk b % nch; its per-lane FP64 sums follow the two stages in shared memory.
+// sample chunk b % nch; each lane adds its nodes' terms to FP64 sums in tensor memory
+// (NormSink), and at its end the block writes one row of partial sums, its warps added
+// in order.  Every wait is bounded: a wait that gives up sets status bit 0, the block
+// stops after the item (all warps leave the loop together), waits with a bound for the
+// copies it issued, frees its tensor memory and returns.
 template <typename T, int V, bool DIFF, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long long n_items) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int stop;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const size_t stage_bytes = (size_t)A.cap_slots * (16 + kSlabStride * sizeof(T));
@@ -379,22 +385,31 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
     const uint32_t bar0 = smem_u32(smem);
     int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
     T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
-    constexpr int kAcc = 4 * V * 32;  // doubles of one warp's norm accumulators
-    double* const nbase = reinterpret_cast<double*>(smem + 16 + 2 * stage_bytes);
-    double* const nacc = A.norm_part ? nbase + warp * kAcc + lane : nullptr;
-    if (nacc) {
-#pragma unroll
-        for (int q = 0; q < 4 * V; ++q) nacc[q * 32] = 0.0;
+    const bool norms = A.norm_part != nullptr;
+    const uint32_t tcols = blockDim.x > 128 ? 64u : 32u;
+    if (warp == 0) {
+        if (norms) tmem_alloc(&tmem_slot, tcols);
+        tmem_relinquish();
     }
     if (threadIdx.x == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
+        stop = 0;
     }
+    if (norms) tmem_fence_before_sync();
     __syncthreads();
+    if (norms) tmem_fence_after_sync();
+    NormSink ns;
+    if (norms) {
+        ns.on = true;
+        ns.tm = tmem_slot + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(warp >> 2) * 32u;
+        norms_zero<V>(ns.tm);
+    }
     long long w = blockIdx.x;
     if (threadIdx.x == 0 && w < n_items) fanp_issue<T>(A, w, bar0, srec0, sslab0);
     const size_t S = (size_t)A.S;
     const T p = step_pressure<T>(A);
+    int stop_it = 0;  // the item at which a wait gave up
     for (int it = 0; w < n_items; w += gridDim.x, ++it) {
         const int sg = it & 1;
         const long long wn = w + gridDim.x;
@@ -423,13 +438,25 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
         // No L2 prefetch ahead here: the prefetching warp's dependent slot-record loads
         // hold its whole block at the item barrier (measured 2.466 -> 3.579 ms/step on the
         // 256x1024 tube with it; node rows alone 3.06 ms).
-        if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
-            if (lane == 0 && A.status) atomicOr(A.status, 1);
-            return;
+        bool ready = true;
+        if (norms) {
+            // warp-uniform, so that the tensor-memory accesses of the epilogue stay converged;
+            // a wait that gives up stops the whole block after this item
+            ready = __all_sync(0xffffffffu, mbar_wait_bounded(bar0 + 8 * sg,
+                                                              (uint32_t)((it >> 1) & 1), kMaxPolls));
+            if (!ready && lane == 0) {
+                if (A.status) atomicOr(A.status, 1);
+                stop = 1;
+            }
+        } else {
+            if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
+                if (lane == 0 && A.status) atomicOr(A.status, 1);
+                return;
+            }
         }
-        if (active) {
+        if (ready && active) {
             if (clamped) {
-                clamp_store<T, V>(A, S, row, nacc, a, col);
+                clamp_store<T, V>(A, S, row, ns, a, col);
             } else {
                 const int kb = __ldg(A.node_ptr + a0);
                 const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
@@ -437,22 +464,45 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
                 ku_row_fan<T, V, DIFF>(stage_rec(srec0, stage_bytes, sg),
                                        stage_slab(sslab0, stage_bytes, sg), k0, k1, A.u, A.coef,
                                        S, col, ua, acc);
-                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f, nacc);
+                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f, ns);
             }
         }
         __syncthreads();
-    }
-    if (A.norm_part) {  // this block's sums over its nodes, warps added in order
-        const int chunk = (int)(blockIdx.x % A.nch);
-        const long long prow = blockIdx.x / A.nch;
-        for (int t = threadIdx.x; t < kAcc; t += blockDim.x) {
-            const int q = t / (32 * V), c = t - q * 32 * V;  // c: sample of the chunk
-            const int ln = c / V, i = c - ln * V;
-            double sum = 0.0;
-            for (int w = 0; w < A.npb; ++w) sum += nbase[w * kAcc + (q * V + i) * 32 + ln];
-            A.norm_part[((size_t)prow * S + (size_t)chunk * 32 * V + c) * 4 + q] = sum;
+        if (norms) {
+            if (*(volatile int*)&stop) {
+                stop_it = it;
+                break;
+            }
         }
     }
+    if (!norms) return;
+    if (*(volatile int*)&stop && threadIdx.x == 0) {
+        // the copies still in flight into this block's stages: the timed-out one and the
+        // one issued for the next item
+        const int sg = stop_it & 1;
+        mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((stop_it >> 1) & 1), kMaxPolls);
+        if (w + gridDim.x < n_items)
+            mbar_wait_bounded(bar0 + 8 * (sg ^ 1), (uint32_t)(((stop_it + 1) >> 1) & 1),
+                              kMaxPolls);
+    }
+    // this block's sums over its nodes, warps added in order, in the (idle) stage memory
+    double* const scr = reinterpret_cast<double*>(smem + 16);
+    for (int wv = 0; wv < A.npb; ++wv) {
+        if (warp == wv) norms_fold<V>(ns.tm, scr + lane, wv == 0);
+        __syncthreads();
+    }
+    const int chunk = (int)(blockIdx.x % A.nch);
+    const long long prow = blockIdx.x / A.nch;
+    for (int t = threadIdx.x; t < 4 * V * 32; t += blockDim.x) {
+        const int q = t / (32 * V), c = t - q * 32 * V;  // c: sample of the chunk
+        const int ln = c / V, i = c - ln * V;
+        A.norm_part[((size_t)prow * S + (size_t)chunk * 32 * V + c) * 4 + q] =
+            scr[(q * V + i) * 32 + ln];
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc(tmem_slot, tcols);
 }
 
 // ------------------------------------------------------------ burst-gather step
@@ -1181,10 +1231,30 @@ int fanp_blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm
         if (e != cudaSuccess)
             return fail(CVFES_ERR_CUDA, "k_step_fanp smem attribute: %s", cudaGetErrorString(e));
     }
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess ||
-        n <= 0)
-        return fail(CVFES_ERR_CUDA, "k_step_fanp: no resident block fits");
+    // From the kernel's registers and shared memory against the SM's budgets.  Not the
+    // occupancy calculator: it reports one block per SM for a kernel that contains a
+    // tensor-memory allocation, whose blocks here give up their allocation permit at
+    // their start and hold 32 or 64 of the SM's 512 columns only when the norms are fused.
+    cudaFuncAttributes fa;
+    CVFES_CUDA_TRY(cudaFuncGetAttributes(&fa, kernel));
+    int regs_sm = 0, smem_sm = 0, reserved = 0, thr_sm = 0, blk_sm = 0;
+    CVFES_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    CVFES_CUDA_TRY(
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CVFES_CUDA_TRY(
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    CVFES_CUDA_TRY(
+        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    CVFES_CUDA_TRY(cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev));
+    const int warps = (threads + 31) / 32;
+    // registers: allocated per warp in units of 256, from the four sub-partitions' quarters
+    const int per_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+    const int by_regs = per_warp > 0 ? 4 * ((regs_sm / 4) / per_warp) / warps : blk_sm;
+    const size_t per_block = fa.sharedSizeBytes + smem + (size_t)reserved;
+    const int by_smem = (int)((size_t)smem_sm / per_block);
+    const int by_thr = thr_sm / (32 * warps);
+    const int n = std::min(std::min(by_regs, by_smem), std::min(by_thr, blk_sm));
+    if (n <= 0) return fail(CVFES_ERR_CUDA, "k_step_fanp: no resident block fits");
     if (n_cache < 32) cache[n_cache++] = Entry{kernel, dev, threads, smem, n};
     *per_sm = n;
     return CVFES_OK;
@@ -1200,6 +1270,12 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
     const int rc = fanp_blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem,
                                       &per_sm);
     if (rc) return rc;
+    // fused norms: each block holds 32 columns of tensor memory (64 above 4 warps), and a
+    // block waits in its allocation until the SM's 512 columns have room
+    if (A.norm_part) {
+        const int cap = threads > 128 ? 8 : 16;
+        if (per_sm > cap) per_sm = cap;
+    }
     long long blocks = (long long)per_sm * sm_count();
     if (blocks > n_items) blocks = n_items;
     if (A.norm_part) {
@@ -1216,20 +1292,14 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
 template <typename T, int V, bool DIFF>
 int launch_fanp(int minb, long long n_items, int threads, size_t smem, cudaStream_t st,
                 const StepArgs<T>& A, long long max_rows = 0, long long* rows = nullptr) {
-    if (A.norm_part) smem += (size_t)A.npb * 4 * V * 32 * sizeof(double);
+    // fused norms: the block's sums are added up in the stage memory at its end
+    const size_t scratch = 16 + (size_t)4 * V * 32 * sizeof(double);
+    if (A.norm_part && smem < scratch) smem = scratch;
     switch (minb) {
-        case 4:
-            return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A,
-                                 max_rows, rows);
-        case 3:
-            return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A,
-                                 max_rows, rows);
-        case 2:
-            return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A,
-                                 max_rows, rows);
-        default:
-            return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A,
-                                 max_rows, rows);
+        case 4: return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A, max_rows, rows);
+        case 3: return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A, max_rows, rows);
+        case 2: return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A, max_rows, rows);
+        default: return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A, max_rows, rows);
     }
 }
 

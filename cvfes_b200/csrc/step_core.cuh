@@ -83,17 +83,164 @@ __device__ __forceinline__ T row_eta(const StepArgs<T>& A, T im) {
 __device__ __forceinline__ float norm_mass(float im) { return im != 0.f ? __frcp_rn(im) : 0.f; }
 __device__ __forceinline__ double norm_mass(double im) { return im != 0.0 ? 1.0 / im : 0.0; }
 
-// Per-lane accumulator of the fused norms: quantity q of sample i of the lane's vector
-// at nacc[(q * V + i) * 32] (lanes innermost: no shared-memory bank conflicts).
+// ------------------------------------------------------------ tensor-memory accumulators
+// The fused norms keep each lane's FP64 sums in tensor memory (TMEM), which the step
+// does not otherwise use: no shared memory (the L1 that serves the neighbour-row
+// gathers) and no registers between nodes.  Warp w of a block owns TMEM lanes
+// 32 (w % 4) .. + 31 and columns from 32 (w / 4); in its lane's row, quantity q (sum u^2,
+// sum du^2, sum m du^2) of sample i is the double at columns 2 (q V + i) and + 1, and
+// the non-finite count of sample i the integer at column 6 V + i.
+struct NormSink {
+    bool on = false;
+    uint32_t tm = 0;  // TMEM address: the lane quarter of the warp and its first column
+};
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {  // warp-wide
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"((uint32_t)__cvta_generic_to_shared(slot)), "r"(cols) : "memory");
+}
+// The block allocates no more tensor memory.  A kernel that contains an allocation gets
+// further blocks on an SM only after its resident blocks have said so (measured on the
+// persistent fan kernel: one block per SM otherwise), so every block says it, whether it
+// allocated or not.
+__device__ __forceinline__ void tmem_relinquish() {  // warp-wide
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {  // warp-wide
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// N consecutive 32-bit columns of the lane's row (32x32b shape: one row per lane).
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[N]) {
+    static_assert(N == 1 || N == 2 || N == 4 || N == 8, "tmem_ld: 1, 2, 4 or 8 columns");
+    if constexpr (N == 1) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];"
+                     : "=r"(r[0]) : "r"(taddr) : "memory");
+    } else if constexpr (N == 2) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                     : "=r"(r[0]), "=r"(r[1]) : "r"(taddr) : "memory");
+    } else if constexpr (N == 4) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr) : "memory");
+    } else {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7])
+            : "r"(taddr)
+            : "memory");
+    }
+}
+template <int N>
+__device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t (&r)[N]) {
+    static_assert(N == 1 || N == 2 || N == 4 || N == 8, "tmem_st: 1, 2, 4 or 8 columns");
+    if constexpr (N == 1) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(r[0])
+                     : "memory");
+    } else if constexpr (N == 2) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr),
+                     "r"(r[0]), "r"(r[1])
+                     : "memory");
+    } else if constexpr (N == 4) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
+                     "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3])
+                     : "memory");
+    } else {
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(
+                taddr),
+            "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+            : "memory");
+    }
+}
+__device__ __forceinline__ void add_to_words(uint32_t& lo, uint32_t& hi, double x) {
+    const double v = __hiloint2double((int)hi, (int)lo) + x;
+    lo = (uint32_t)__double2loint(v);
+    hi = (uint32_t)__double2hiint(v);
+}
+
+// Zero the lane's accumulators (every thread of the warp calls it).
+template <int V>
+__device__ __forceinline__ void norms_zero(uint32_t tm) {
+    uint32_t z[2 * V], zn[V];
+#pragma unroll
+    for (int i = 0; i < 2 * V; ++i) z[i] = 0u;
+#pragma unroll
+    for (int i = 0; i < V; ++i) zn[i] = 0u;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) tmem_st<2 * V>(tm + (uint32_t)(q * 2 * V), z);
+    tmem_st<V>(tm + (uint32_t)(6 * V), zn);
+    tmem_wait_st();
+}
+
+// Add one node's terms to the lane's accumulators (every thread of the warp calls it).
 template <typename T, int V>
-__device__ __forceinline__ void norms_add(double* nacc, const Vec<T, V>& im, const T (&su)[V],
+__device__ __forceinline__ void norms_add(uint32_t tm, const Vec<T, V>& im, const T (&su)[V],
                                           const T (&sv)[V], const int (&nf)[V]) {
+    tmem_wait_st();  // the previous node's stores to these columns
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {  // one quantity at a time: 2V registers in flight
+        uint32_t r[2 * V];
+        tmem_ld<2 * V>(tm + (uint32_t)(q * 2 * V), r);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const T x = q == 0 ? su[i] : (q == 1 ? sv[i] : norm_mass(im.v[i]) * sv[i]);
+            add_to_words(r[2 * i], r[2 * i + 1], (double)x);
+        }
+        tmem_st<2 * V>(tm + (uint32_t)(q * 2 * V), r);
+    }
+    int any = 0;
+#pragma unroll
+    for (int i = 0; i < V; ++i) any |= nf[i];
+    if (__any_sync(0xffffffffu, any != 0)) {  // rare: a non-finite value in the warp's node
+        uint32_t rn[V];
+        tmem_ld<V>(tm + (uint32_t)(6 * V), rn);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < V; ++i) rn[i] += (uint32_t)nf[i];
+        tmem_st<V>(tm + (uint32_t)(6 * V), rn);
+    }
+}
+
+// Add the lane's sums to dst[(q V + i) * 32] (quantity q of sample i; q = 3 the non-finite
+// count), or store them there when first; one quantity at a time (every thread of the
+// warp calls it).
+template <int V>
+__device__ __forceinline__ void norms_fold(uint32_t tm, double* dst, bool first) {
+    tmem_wait_st();
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        uint32_t r[2 * V];
+        tmem_ld<2 * V>(tm + (uint32_t)(q * 2 * V), r);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            double* c = dst + (q * V + i) * 32;
+            const double x = __hiloint2double((int)r[2 * i + 1], (int)r[2 * i]);
+            *c = first ? x : *c + x;
+        }
+    }
+    uint32_t rn[V];
+    tmem_ld<V>(tm + (uint32_t)(6 * V), rn);
+    tmem_wait_ld();
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-        nacc[(0 * V + i) * 32] += (double)su[i];
-        nacc[(1 * V + i) * 32] += (double)sv[i];
-        nacc[(2 * V + i) * 32] += (double)(norm_mass(im.v[i]) * sv[i]);
-        if (nf[i]) nacc[(3 * V + i) * 32] += (double)nf[i];
+        double* c = dst + (3 * V + i) * 32;
+        *c = first ? (double)rn[i] : *c + (double)rn[i];
     }
 }
 
@@ -350,10 +497,10 @@ __device__ __forceinline__ void step_update(const StepArgs<T>& A, size_t S, size
 }
 
 // Dirichlet row: u_{n+1} = clamp; in the velocity-state form also v_{n+1} = clamp - u_n.
-// With nacc (fused norms) the row's contributions are added there.
+// With ns.on (fused norms) the row's contributions are added to the lane's accumulators.
 template <typename T, int V>
 __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size_t row,
-                                            double* nacc = nullptr, long long a = 0,
+                                            NormSink ns = NormSink(), long long a = 0,
                                             size_t col = 0) {
     const Vec<T, V> cl = vfill<T, V>(A.clamp);
     T su[V], sv[V];
@@ -365,10 +512,10 @@ __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        if (A.vel || nacc) {
+        if (A.vel || ns.on) {
             const Vec<T, V> dv = vsub(cl, ldg<T, V>(A.u + row + d * S));
             if (A.vel) stcs<T, V>(A.vel + row + d * S, dv);
-            if (nacc) {
+            if (ns.on) {
 #pragma unroll
                 for (int i = 0; i < V; ++i) {
                     su[i] = fma(cl.v[i], cl.v[i], su[i]);
@@ -379,17 +526,17 @@ __device__ __forceinline__ void clamp_store(const StepArgs<T>& A, size_t S, size
         }
         stcs<T, V>(A.un + row + d * S, cl);
     }
-    if (nacc) norms_add<T, V>(nacc, ldcs<T, V>(A.invm + (size_t)a * S + col), su, sv, nf);
+    if (ns.on) norms_add<T, V>(ns.tm, ldcs<T, V>(A.invm + (size_t)a * S + col), su, sv, nf);
 }
 
 // As step_update, reading the row's u_{n-1} (or v_n) and inverse mass here.
-// With nacc (fused norms) the row's contributions to the per-sample sums of u_{n+1}^2,
+// With ns.on (fused norms) the row's contributions to the per-sample sums of u_{n+1}^2,
 // du^2 (v_{n+1}^2, or u_{n+1} - u_n) and m du^2 are added there (node terms as norms_add).
 template <typename T, int V>
 __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a, size_t S,
                                               size_t col, size_t row, const Vec<T, V> (&ua)[3],
                                               const Vec<T, V> (&acc)[3], const T (&f)[3],
-                                              double* nacc = nullptr) {
+                                              NormSink ns = NormSink()) {
     const Vec<T, V> im = ldcs<T, V>(A.invm + (size_t)a * S + col);
     T su[V], sv[V];
     int nf[V];
@@ -413,7 +560,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
                 const bool live = im.v[i] != T(0);
                 o.v[i] = live ? ua[d].v[i] + v : T(0);
                 vn.v[i] = live ? v : -ua[d].v[i];
-                if (nacc) {
+                if (ns.on) {
                     su[i] = fma(o.v[i], o.v[i], su[i]);
                     sv[i] = fma(vn.v[i], vn.v[i], sv[i]);
                     nf[i] += isfinite(o.v[i]) ? 0 : 1;
@@ -422,7 +569,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
             stcs<T, V>(A.un + row + d * S, o);
             stcs<T, V>(A.vel + row + d * S, vn);
         }
-        if (nacc) norms_add<T, V>(nacc, im, su, sv, nf);
+        if (ns.on) norms_add<T, V>(ns.tm, im, su, sv, nf);
         return;
     }
 #pragma unroll
@@ -436,7 +583,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
             const T w = A.w0 * im.v[i];
             const T v = fma(w, load - acc[d].v[i], fma(-row_eta(A, im.v[i]), dv, dv));
             o.v[i] = (im.v[i] != T(0)) ? ua[d].v[i] + v : T(0);
-            if (nacc) {
+            if (ns.on) {
                 const T du = o.v[i] - ua[d].v[i];
                 su[i] = fma(o.v[i], o.v[i], su[i]);
                 sv[i] = fma(du, du, sv[i]);
@@ -445,7 +592,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs<T>& A, long long a,
         }
         stcs<T, V>(A.un + row + d * S, o);
     }
-    if (nacc) norms_add<T, V>(nacc, im, su, sv, nf);
+    if (ns.on) norms_add<T, V>(ns.tm, im, su, sv, nf);
 }
 
 // ------------------------------------------------------------ fan-rotation row
