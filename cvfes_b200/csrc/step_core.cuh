@@ -75,12 +75,19 @@ __device__ __forceinline__ T row_eta(const StepArgs<T>& A, T im) {
 // Norm terms of one node (sum of squares of its three new values, of its three
 // increments, and the count of non-finite values) are formed in the state's type and
 // only the node sums are taken to FP64: with the FP32 state each node term carries
-// three FP32 roundings (five for the mass-weighted one: <= 3e-7 relative, all terms
-// positive, so the sum over nodes keeps that bound), and the FP64 sums
+// three FP32 roundings (the mass-weighted one also a reciprocal of at most 1 ulp and a
+// product: <= 4e-7 relative; all terms positive, so the sum over nodes keeps the
+// bound), and the FP64 sums
 // over nodes need three conversions per node instead of seven (a conversion to FP64
 // runs at a quarter of the FP64 rate; per value they cost a tenth of the step).  The
 // separate norms pass forms the same node terms in the same order.
-__device__ __forceinline__ float norm_mass(float im) { return im != 0.f ? __frcp_rn(im) : 0.f; }
+// FP32: the hardware reciprocal approximation (rcp.approx, at most 1 ulp), one instruction
+// where the correctly rounded reciprocal cost 4% of the step as a norm term.
+__device__ __forceinline__ float norm_mass(float im) {
+    float m;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(m) : "f"(im));
+    return im != 0.f ? m : 0.f;
+}
 __device__ __forceinline__ double norm_mass(double im) { return im != 0.0 ? 1.0 / im : 0.0; }
 
 // ------------------------------------------------------------ tensor-memory accumulators
@@ -190,18 +197,19 @@ __device__ __forceinline__ void norms_zero(uint32_t tm) {
 template <typename T, int V>
 __device__ __forceinline__ void norms_add(uint32_t tm, const Vec<T, V>& im, const T (&su)[V],
                                           const T (&sv)[V], const int (&nf)[V]) {
+    uint32_t r[3][2 * V];
     tmem_wait_st();  // the previous node's stores to these columns
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {  // one quantity at a time: 2V registers in flight
-        uint32_t r[2 * V];
-        tmem_ld<2 * V>(tm + (uint32_t)(q * 2 * V), r);
-        tmem_wait_ld();
+    for (int q = 0; q < 3; ++q) tmem_ld<2 * V>(tm + (uint32_t)(q * 2 * V), r[q]);
+    tmem_wait_ld();
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
 #pragma unroll
         for (int i = 0; i < V; ++i) {
             const T x = q == 0 ? su[i] : (q == 1 ? sv[i] : norm_mass(im.v[i]) * sv[i]);
-            add_to_words(r[2 * i], r[2 * i + 1], (double)x);
+            add_to_words(r[q][2 * i], r[q][2 * i + 1], (double)x);
         }
-        tmem_st<2 * V>(tm + (uint32_t)(q * 2 * V), r);
+        tmem_st<2 * V>(tm + (uint32_t)(q * 2 * V), r[q]);
     }
     int any = 0;
 #pragma unroll

@@ -345,7 +345,8 @@ int cvfes_solid_init_f32(const cvfes_solid_mesh* mesh, const float* coef, const 
  *                   count of non-finite values.
  * Sums over nodes are FP64; each node's term (its three values) is formed in the
  * state's type: FP32 terms carry three FP32 roundings (<= 1.8e-7 relative; the
- * mass-weighted term five, <= 3e-7), FP64 terms FP64 ones.
+ * mass-weighted term also a reciprocal of at most 1 ulp and a product, <= 4e-7), FP64
+ * terms FP64 ones.
  *   work f64, at least cvfes_norms_work_size(N, S) doubles (block partials).
  * Returns CVFES_ERR_NONFINITE (after writing out) when any value is NaN/Inf
  * and check_finite != 0 (this synchronises the stream).                       */

@@ -201,7 +201,8 @@ def test_norms_and_watchdog(lib, cuda):
 def test_fp32_norms_against_fp64_sums(lib, cuda, state, norms_every):
     """FP32 state, separate pass and fused into the step: the norms against FP64 sums of
     the same FP32 values.  Each node's three-value term is formed in FP32 (three
-    roundings; five for the mass-weighted term), so the bound is 2e-7 (3e-7)."""
+    roundings; the mass-weighted term also a reciprocal of at most 1 ulp and a product),
+    so the bound is 2e-7 (4e-7)."""
     from cvfes_b200.cases import CASES
     case = CASES["tube64x128"]
     mesh = c0_mesh(64)
@@ -220,7 +221,7 @@ def test_fp32_norms_against_fp64_sums(lib, cuda, state, norms_every):
     m = np.repeat(np.where(im != 0, 1.0 / np.where(im != 0, im, 1.0), 0.0), 3, axis=0)
     np.testing.assert_allclose(nrm[:, 0], (u ** 2).sum(0), rtol=2e-7, atol=0)
     np.testing.assert_allclose(nrm[:, 1], (du ** 2).sum(0), rtol=2e-7, atol=0)
-    np.testing.assert_allclose(nrm[:, 2], (m * du ** 2).sum(0), rtol=3e-7, atol=0)
+    np.testing.assert_allclose(nrm[:, 2], (m * du ** 2).sum(0), rtol=4e-7, atol=0)
     assert np.all(nrm[:, 3] == 0)
 
 
