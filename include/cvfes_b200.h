@@ -288,9 +288,10 @@ int cvfes_solid_step_f32(const cvfes_solid_mesh* mesh, const float* coef, const 
 /* One step as cvfes_solid_step_* and, in the same pass, the FP64 per-sample norms of the
  * new state (out f64 [S][4] as cvfes_solid_norms_*: sum u_next^2, sum du^2, sum m du^2,
  * non-finite count, du = u_next - u, or the new increment in the velocity-state form).
- * The persistent fan kernel accumulates the sums per block in shared memory while it
- * writes the state, so the state is not read a second time; shapes without it (S / vec
- * not a multiple of 32, no max_degree) run the step and the separate norms pass.
+ * The persistent fan kernel accumulates each lane's sums in tensor memory (32 or 64
+ * columns per block, freed at its end) while it writes the state, so the state is not
+ * read a second time; shapes without it (S / vec not a multiple of 32, no max_degree)
+ * run the step and the separate norms pass.
  * work: cvfes_norms_work_size(N, S) doubles.  check_finite: as cvfes_solid_norms_*.
  * out_host (NULL, or S*4 doubles of pinned host memory): when given, the call also copies
  * out to out_host, reads and clears mesh->status (CVFES_ERR_TIMEOUT if a bounded wait
