@@ -226,7 +226,7 @@ __device__ __forceinline__ void load27(const T* K, T (&kk)[27]) {
 // Gamma_e += dchi^T Khat_e du for the element owned by this slot: (u1, u2) and (x1, x2) are
 // the first and second neighbour rows of u_n and chi_{n+1}, already differences
 // u_b - u_a in the DIFF form, raw rows otherwise.
-template <typename T, int V, bool DIFF>
+template <typename T, int V, bool DIFF, bool SMEM_OWN = false>
 __device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, const T* own, size_t S,
                                            size_t col,
                                            const Vec<T, V> (&u1)[3], const Vec<T, V> (&u2)[3],
@@ -247,11 +247,13 @@ __device__ __forceinline__ void owner_grad(const RevArgs<T>& A, int e, const T* 
             dy2[d] = vsub(x2[d], ca[d]);
         }
     }
-    // own points into global memory (gather kernel) or shared memory (fan kernel): plain
-    // generic loads, not the global-only read-only path
-    T ob[27];
-#pragma unroll
-    for (int i = 0; i < 27; ++i) ob[i] = own[i];
+    // own points into global memory (gather kernel) or shared memory (fan kernel, SMEM_OWN):
+    // plain generic loads, not the global-only read-only path.  From shared memory they
+    // are volatile, so that each of the 27 values is read where it is used instead of all
+    // of them being hoisted into registers beside the three rotating neighbour-row sets
+    // (the fan kernel spilled at its 128-register cap with them hoisted; it fits without).
+    using OwnPtr = typename std::conditional<SMEM_OWN, const volatile T*, const T*>::type;
+    const OwnPtr ob = own;
     Vec<T, V> g = vzero<T, V>();
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -509,7 +511,7 @@ __device__ __forceinline__ void rev_phase(int& k, int k1, const int4* srec, cons
     slot_fma2<T, V, DIFF>(sslab + (size_t)kSlabStride * k, ccur, pu, cu, px, cx, ua, ca, accU,
                           accC);
     if (((r.w >> 8) & 3) == 0)
-        owner_grad<T, V, DIFF>(A, r.x, sown + (size_t)kOwnStride * k, S, col, pu, cu, px, cx, ua,
+        owner_grad<T, V, DIFF, true>(A, r.x, sown + (size_t)kOwnStride * k, S, col, pu, cu, px, cx, ua,
                                ca);
     if (more && !(rn.w & 1)) {  // fan break: the next slot's first neighbour is new
         load3<T, V>(cu, A.u, rn.y, S, col);
