@@ -146,6 +146,7 @@ SIGNATURES = {
     "cvfes_get_step_prefetch": (C.c_int, [I32, P, P]),
     "cvfes_status_read": (C.c_int, [P, P]),
     "cvfes_set_wait_probe": (C.c_int, [I32]),
+    "cvfes_set_norms_memory": (C.c_int, [I32]),
     "cvfes_batch_table_bytes": (C.c_int64, [I32]),
     "cvfes_batch_pack": (C.c_int, [C.POINTER(BatchItem), I32, I32, I32, P, P]),
     "cvfes_batch_step": (C.c_int, [P, I32, P, I32, I32, I32, I32, P, I64, I32, P]),

@@ -776,7 +776,7 @@ struct RevTuning {
 // FP64 on the 64x128 tube with 64 samples (reverse pass of 500 steps: vec 1 with 4 nodes
 // per block 29.6 ms, vec 2 with 2 nodes 30.6 ms, persistent 30.2 ms).
 static RevTuning g_rev32 = {2, 2, 1, 2};
-static RevTuning g_rev64 = {1, 4, 1, 2};
+static RevTuning g_rev64 = {1, 4, 2, 2};
 template <typename T>
 RevTuning& rev_tuning() {
     return sizeof(T) == 4 ? g_rev32 : g_rev64;

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <type_traits>
 
@@ -367,14 +368,105 @@ __device__ __forceinline__ void fanp_issue(const StepArgs<T>& A, long long w, ui
     bulk_g2s(smem_u32(sslab), A.slab + (size_t)kb * kSlabStride, b_slab, bar);
 }
 
-// With A.norm_part (fused norms) the grid is a multiple of nch, so block b always has
-// sample chunk b % nch; each lane adds its nodes' terms to FP64 sums in tensor memory
-// (NormSink), and at its end the block writes one row of partial sums, its warps added
-// in order.  Every wait is bounded: a wait that gives up sets status bit 0, the block
+// With A.norm_part (fused norms, shared-memory mode) the grid is a multiple of nch, so
+// block b always has sample chunk b % nch; its per-lane FP64 sums follow the two stages
+// in shared memory.  Without norms this is the plain persistent step.
+template <typename T, int V, bool DIFF, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long long n_items) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const size_t stage_bytes = (size_t)A.cap_slots * (16 + kSlabStride * sizeof(T));
+    // stage q: barrier at smem + 8q, records then stiffness rows at smem + 16 + q * stage_bytes
+    const uint32_t bar0 = smem_u32(smem);
+    int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
+    T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
+    constexpr int kAcc = 4 * V * 32;  // doubles of one warp's norm accumulators
+    double* const nbase = reinterpret_cast<double*>(smem + 16 + 2 * stage_bytes);
+    double* const nacc = A.norm_part ? nbase + warp * kAcc + lane : nullptr;
+    if (nacc) {
+#pragma unroll
+        for (int q = 0; q < 4 * V; ++q) nacc[q * 32] = 0.0;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+    }
+    __syncthreads();
+    long long w = blockIdx.x;
+    if (threadIdx.x == 0 && w < n_items) fanp_issue<T>(A, w, bar0, srec0, sslab0);
+    const size_t S = (size_t)A.S;
+    const T p = step_pressure<T>(A);
+    for (int it = 0; w < n_items; w += gridDim.x, ++it) {
+        const int sg = it & 1;
+        const long long wn = w + gridDim.x;
+        if (threadIdx.x == 0 && wn < n_items)
+            fanp_issue<T>(A, wn, bar0 + 8 * (sg ^ 1), stage_rec(srec0, stage_bytes, sg ^ 1), stage_slab(sslab0, stage_bytes, sg ^ 1));
+        const long long nb = w / A.nch;
+        const int chunk = (int)(w - nb * A.nch);
+        const long long a0 = nb * A.npb;
+        const long long a1 = (a0 + A.npb < A.n_nodes) ? a0 + A.npb : A.n_nodes;
+        const long long a = a0 + warp;
+        const bool active = warp < A.npb && a < a1;
+        const size_t col = ((size_t)chunk * 32 + lane) * V;
+        const size_t row = (size_t)a * 3 * S + col;
+        const bool clamped = a < A.n_clamped;
+        Vec<T, V> ua[3];
+        T f[3];
+        if (active && !clamped) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ua[d] = ldg<T, V>(A.u + row + d * S);
+                prefetch_l2(A.up + row + d * S);
+            }
+            prefetch_l2(A.invm + (size_t)a * S + col);
+            node_load<T>(A, a, p, f);
+        }
+        // No L2 prefetch ahead here: the prefetching warp's dependent slot-record loads
+        // hold its whole block at the item barrier (measured 2.466 -> 3.579 ms/step on the
+        // 256x1024 tube with it; node rows alone 3.06 ms).
+        if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
+            if (lane == 0 && A.status) atomicOr(A.status, 1);
+            return;
+        }
+        if (active) {
+            if (clamped) {
+                clamp_store<T, V>(A, S, row, nacc, a, col);
+            } else {
+                const int kb = __ldg(A.node_ptr + a0);
+                const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
+                Vec<T, V> acc[3];
+                ku_row_fan<T, V, DIFF>(stage_rec(srec0, stage_bytes, sg),
+                                       stage_slab(sslab0, stage_bytes, sg), k0, k1, A.u, A.coef,
+                                       S, col, ua, acc);
+                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f, nacc);
+            }
+        }
+        __syncthreads();
+    }
+    if (A.norm_part) {  // this block's sums over its nodes, warps added in order
+        const int chunk = (int)(blockIdx.x % A.nch);
+        const long long prow = blockIdx.x / A.nch;
+        for (int t = threadIdx.x; t < kAcc; t += blockDim.x) {
+            const int q = t / (32 * V), c = t - q * 32 * V;  // c: sample of the chunk
+            const int ln = c / V, i = c - ln * V;
+            double sum = 0.0;
+            for (int w = 0; w < A.npb; ++w) sum += nbase[w * kAcc + (q * V + i) * 32 + ln];
+            A.norm_part[((size_t)prow * S + (size_t)chunk * 32 * V + c) * 4 + q] = sum;
+        }
+    }
+}
+
+// The persistent step with the norms fused in (tensor-memory mode, the default): the
+// grid is a multiple of nch, so block b always has sample chunk b % nch; each lane adds
+// its nodes' terms to FP64 sums in tensor memory (norms_add), and at its end the block
+// writes one row of partial sums, its warps added in order.  A kernel of its own: the
+// plain step without any tensor-memory instruction is 6% faster (2.30 against 2.44
+// ms/step on the 256x1024 tube, and 7.2 against 8.1 ms for 500 steps of the 64x128 tube).  Every wait is bounded: a wait that gives up sets status bit 0, the block
 // stops after the item (all warps leave the loop together), waits with a bound for the
 // copies it issued, frees its tensor memory and returns.
 template <typename T, int V, bool DIFF, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long long n_items) {
+__global__ void __launch_bounds__(256, MINB) k_step_fanp_tm(StepArgs<T> A, long long n_items) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t tmem_slot;
     __shared__ int stop;
@@ -385,10 +477,9 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
     const uint32_t bar0 = smem_u32(smem);
     int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
     T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)A.cap_slots * 16);
-    const bool norms = A.norm_part != nullptr;
     const uint32_t tcols = blockDim.x > 128 ? 64u : 32u;
     if (warp == 0) {
-        if (norms) tmem_alloc(&tmem_slot, tcols);
+        tmem_alloc(&tmem_slot, tcols);
         tmem_relinquish();
     }
     if (threadIdx.x == 0) {
@@ -396,15 +487,13 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
         mbar_init(bar0 + 8, 1);
         stop = 0;
     }
-    if (norms) tmem_fence_before_sync();
+    tmem_fence_before_sync();
     __syncthreads();
-    if (norms) tmem_fence_after_sync();
-    NormSink ns;
-    if (norms) {
-        ns.on = true;
-        ns.tm = tmem_slot + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(warp >> 2) * 32u;
-        norms_zero<V>(ns.tm);
-    }
+    tmem_fence_after_sync();
+    // this lane's TMEM row: the warp's lane quarter and, above 4 warps, the second 32 columns
+    const uint32_t tm =
+        tmem_slot + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(warp >> 2) * 32u;
+    norms_zero<V>(tm);
     long long w = blockIdx.x;
     if (threadIdx.x == 0 && w < n_items) fanp_issue<T>(A, w, bar0, srec0, sslab0);
     const size_t S = (size_t)A.S;
@@ -438,25 +527,17 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
         // No L2 prefetch ahead here: the prefetching warp's dependent slot-record loads
         // hold its whole block at the item barrier (measured 2.466 -> 3.579 ms/step on the
         // 256x1024 tube with it; node rows alone 3.06 ms).
-        bool ready = true;
-        if (norms) {
-            // warp-uniform, so that the tensor-memory accesses of the epilogue stay converged;
-            // a wait that gives up stops the whole block after this item
-            ready = __all_sync(0xffffffffu, mbar_wait_bounded(bar0 + 8 * sg,
-                                                              (uint32_t)((it >> 1) & 1), kMaxPolls));
-            if (!ready && lane == 0) {
-                if (A.status) atomicOr(A.status, 1);
-                stop = 1;
-            }
-        } else {
-            if (!mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls)) {
-                if (lane == 0 && A.status) atomicOr(A.status, 1);
-                return;
-            }
+        // warp-uniform, so that the tensor-memory accesses of the epilogue stay converged;
+        // a wait that gives up stops the whole block after this item
+        const bool ready = __all_sync(
+            0xffffffffu, mbar_wait_bounded(bar0 + 8 * sg, (uint32_t)((it >> 1) & 1), kMaxPolls));
+        if (!ready && lane == 0) {
+            if (A.status) atomicOr(A.status, 1);
+            stop = 1;
         }
         if (ready && active) {
             if (clamped) {
-                clamp_store<T, V>(A, S, row, ns, a, col);
+                clamp_store_tm<T, V>(A, S, row, tm, a, col);
             } else {
                 const int kb = __ldg(A.node_ptr + a0);
                 const int k0 = __ldg(A.node_ptr + a) - kb, k1 = __ldg(A.node_ptr + a + 1) - kb;
@@ -464,18 +545,15 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
                 ku_row_fan<T, V, DIFF>(stage_rec(srec0, stage_bytes, sg),
                                        stage_slab(sslab0, stage_bytes, sg), k0, k1, A.u, A.coef,
                                        S, col, ua, acc);
-                step_epilogue<T, V>(A, a, S, col, row, ua, acc, f, ns);
+                step_epilogue_tm<T, V>(A, a, S, col, row, ua, acc, f, tm);
             }
         }
         __syncthreads();
-        if (norms) {
-            if (*(volatile int*)&stop) {
-                stop_it = it;
-                break;
-            }
+        if (*(volatile int*)&stop) {
+            stop_it = it;
+            break;
         }
     }
-    if (!norms) return;
     if (*(volatile int*)&stop && threadIdx.x == 0) {
         // the copies still in flight into this block's stages: the timed-out one and the
         // one issued for the next item
@@ -488,7 +566,7 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
     // this block's sums over its nodes, warps added in order, in the (idle) stage memory
     double* const scr = reinterpret_cast<double*>(smem + 16);
     for (int wv = 0; wv < A.npb; ++wv) {
-        if (warp == wv) norms_fold<V>(ns.tm, scr + lane, wv == 0);
+        if (warp == wv) norms_fold<V>(tm, scr + lane, wv == 0);
         __syncthreads();
     }
     const int chunk = (int)(blockIdx.x % A.nch);
@@ -1260,6 +1338,10 @@ int fanp_blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm
     return CVFES_OK;
 }
 
+// Where the fused norms keep their sums: 0 tensor memory (k_step_fanp_tm), 1 shared memory
+// (k_step_fanp).  Both give bitwise the same norms.
+static std::atomic<int> g_norms_mode{0};
+
 // The persistent fan kernel on as many blocks as are resident (at most one per work
 // item).  With fused norms the grid is rounded down to a multiple of the sample chunks
 // and capped at max_rows chunks' worth, and *rows gets the partial rows written.
@@ -1270,9 +1352,9 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
     const int rc = fanp_blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem,
                                       &per_sm);
     if (rc) return rc;
-    // fused norms: each block holds 32 columns of tensor memory (64 above 4 warps), and a
-    // block waits in its allocation until the SM's 512 columns have room
-    if (A.norm_part) {
+    // fused norms in tensor memory: each block holds 32 columns (64 above 4 warps), and
+    // a block waits in its allocation until the SM's 512 columns have room
+    if (A.norm_part && g_norms_mode.load() == 0) {
         const int cap = threads > 128 ? 8 : 16;
         if (per_sm > cap) per_sm = cap;
     }
@@ -1292,15 +1374,24 @@ int launch_fanp_k(K kernel, long long n_items, int threads, size_t smem, cudaStr
 template <typename T, int V, bool DIFF>
 int launch_fanp(int minb, long long n_items, int threads, size_t smem, cudaStream_t st,
                 const StepArgs<T>& A, long long max_rows = 0, long long* rows = nullptr) {
-    // fused norms: the block's sums are added up in the stage memory at its end
-    const size_t scratch = 16 + (size_t)4 * V * 32 * sizeof(double);
-    if (A.norm_part && smem < scratch) smem = scratch;
-    switch (minb) {
-        case 4: return launch_fanp_k(k_step_fanp<T, V, DIFF, 4>, n_items, threads, smem, st, A, max_rows, rows);
-        case 3: return launch_fanp_k(k_step_fanp<T, V, DIFF, 3>, n_items, threads, smem, st, A, max_rows, rows);
-        case 2: return launch_fanp_k(k_step_fanp<T, V, DIFF, 2>, n_items, threads, smem, st, A, max_rows, rows);
-        default: return launch_fanp_k(k_step_fanp<T, V, DIFF, 1>, n_items, threads, smem, st, A, max_rows, rows);
+#define CVFES_FANP_K(K, MB) launch_fanp_k(K<T, V, DIFF, MB>, n_items, threads, smem, st, A, max_rows, rows)
+#define CVFES_FANP(K)                                   \
+    switch (minb) {                                     \
+        case 4: return CVFES_FANP_K(K, 4);              \
+        case 3: return CVFES_FANP_K(K, 3);              \
+        case 2: return CVFES_FANP_K(K, 2);              \
+        default: return CVFES_FANP_K(K, 1);             \
     }
+    if (A.norm_part && g_norms_mode.load() == 0) {
+        // the block's sums are added up in the (idle) stage memory at its end
+        const size_t scratch = 16 + (size_t)4 * V * 32 * sizeof(double);
+        if (smem < scratch) smem = scratch;
+        CVFES_FANP(k_step_fanp_tm)
+    }
+    if (A.norm_part) smem += (size_t)A.npb * 4 * V * 32 * sizeof(double);
+    CVFES_FANP(k_step_fanp)
+#undef CVFES_FANP
+#undef CVFES_FANP_K
 }
 
 template <typename T, int V, bool DIFF, int MAXD>
@@ -1956,6 +2047,13 @@ extern "C" int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int
     const int q = precision == 32 ? 0 : 1;
     if (distance) *distance = g_pf_dist[q];
     if (parts) *parts = g_pf_parts[q];
+    return CVFES_OK;
+}
+
+extern "C" int cvfes_set_norms_memory(int32_t mode) {
+    if (mode != 0 && mode != 1)
+        return fail(CVFES_ERR_ARG, "cvfes_set_norms_memory: mode must be 0 (tensor) or 1 (shared)");
+    g_norms_mode = mode;
     return CVFES_OK;
 }
 

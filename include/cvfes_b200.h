@@ -148,6 +148,13 @@ int cvfes_get_step_prefetch(int32_t precision, int32_t* distance, int32_t* parts
  * it off.  Applies to launches made after the call (graphs keep what they captured). */
 int cvfes_set_wait_probe(int32_t polls);
 
+/* Where a step with the norms fused in (cvfes_solid_step_norms_*) keeps each lane's sums:
+ * 0 (default) tensor memory, in a kernel of its own; 1 shared memory, in the plain
+ * persistent kernel (16 KB more per block at 4 nodes per block and 4 samples per
+ * thread, taken from the L1 of the neighbour-row gathers).  Both give bitwise the
+ * same norms.                                                                       */
+int cvfes_set_norms_memory(int32_t mode);
+
 /* Read and clear the device status word of a mesh descriptor (synchronises the
  * stream).  Returns CVFES_ERR_TIMEOUT if a bounded device wait gave up since
  * the last read, else CVFES_OK.                                               */

@@ -52,6 +52,9 @@ def test_tuning_setters_validate_and_round_trip(lib):
             assert lib.cvfes_set_step_tuning(*bad) == _lib.CVFES_ERR_ARG
         assert lib.cvfes_set_wait_probe(-1) == _lib.CVFES_ERR_ARG
         assert lib.cvfes_set_wait_probe(0) == _lib.CVFES_OK
+        assert lib.cvfes_set_norms_memory(2) == _lib.CVFES_ERR_ARG
+        assert lib.cvfes_set_norms_memory(1) == _lib.CVFES_OK
+        assert lib.cvfes_set_norms_memory(0) == _lib.CVFES_OK
     finally:
         _lib.set_step_prefetch(32, **saved)
     t = _lib.get_step_tuning(64)

@@ -594,6 +594,33 @@ def test_fused_step_norms_match_separate_pass(lib, cuda, precision, state, S):
     assert torch.equal(fused.local_displacement(), plain.local_displacement())
 
 
+@pytest.mark.parametrize("precision,state", [(32, "velocity"), (64, "previous")])
+def test_norms_memory_modes_agree_bitwise(lib, cuda, precision, state):
+    """The fused norms kept in tensor memory (default) and in shared memory
+    (cvfes_set_norms_memory(1)): the same state and bitwise the same norms."""
+    from cvfes_b200.cases import CASES
+    case = CASES["tube64x128"]
+    mesh = c0_mesh(128)
+    pres = case.pressures(12)
+    runs = []
+    try:
+        for mode in (0, 1):
+            call("cvfes_set_norms_memory", mode)
+            s = GPUSolidSolver(LocalComm(), mesh, Cfg(case.dt, 128, precision, chunk=12,
+                                                      state=state, norms_every=1))
+            out = []
+            for n in range(12):
+                s.pressure = float(pres[n])
+                s.Solve(None, case.dt)
+                out.append(s.Norms())
+            assert s._norms_step == s.step_count
+            runs.append((s.local_displacement().clone(), np.stack(out)))
+    finally:
+        call("cvfes_set_norms_memory", 0)
+    assert torch.equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
 @pytest.mark.parametrize("precision", [64, 32])
 def test_opencl_semantics_against_restatement(lib, cuda, precision):
     """[gpu] semantics = opencl (the OpenCL class's numerics: mean(E h) over the element's
