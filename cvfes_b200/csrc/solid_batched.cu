@@ -149,12 +149,14 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchMesh* __restric
 }
 
 
-// Stage the slot records and stiffness rows of fan item w into (srec, sslab).
+// Stage the slot records and stiffness rows of fan item w into (srec, sslab); returns the
+// item's mesh.
 template <typename T>
-__device__ __forceinline__ void batch_fan_issue(const BatchMesh* __restrict__ tab, int n_meshes,
-                                                long long w, int cap, uint32_t bar, int4* srec,
-                                                T* sslab) {
-    const BatchMesh& M = tab[batch_mesh_of(tab, n_meshes, w, true)];
+__device__ __forceinline__ int batch_fan_issue(const BatchMesh* __restrict__ tab, int n_meshes,
+                                               long long w, int cap, uint32_t bar, int4* srec,
+                                               T* sslab) {
+    const int m = batch_mesh_of(tab, n_meshes, w, true);
+    const BatchMesh& M = tab[m];
     const long long nb = (w - M.f_off) / M.f_chunks;
     const long long a0 = nb * (long long)(kBatchWarps * M.f_npw);
     long long a1 = a0 + kBatchWarps * M.f_npw;
@@ -163,7 +165,7 @@ __device__ __forceinline__ void batch_fan_issue(const BatchMesh* __restrict__ ta
     const int nsl = ke - kb;
     if (nsl <= 0 || nsl > cap) {
         mbar_arrive_expect_tx(bar, 0);
-        return;
+        return m;
     }
     const uint32_t b_rec = (uint32_t)nsl * 16u;
     const uint32_t b_slab = (uint32_t)nsl * (uint32_t)(kSlabStride * sizeof(T));
@@ -171,6 +173,7 @@ __device__ __forceinline__ void batch_fan_issue(const BatchMesh* __restrict__ ta
     bulk_g2s(smem_u32(srec), M.rec + kb, b_rec, bar);
     bulk_g2s(smem_u32(sslab), static_cast<const T*>(M.slab) + (size_t)kb * kSlabStride, b_slab,
              bar);
+    return m;
 }
 
 template <typename T, int V, bool DIFF, int MINB>
@@ -186,6 +189,9 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
     const uint32_t bar0 = smem_u32(smem);
     int4* const srec0 = reinterpret_cast<int4*>(smem + 16);
     T* const sslab0 = reinterpret_cast<T*>(smem + 16 + (size_t)cap * 16);
+    // the mesh of the item in each stage, found by thread 0 when it issues the item's copies
+    // (one binary search per item instead of one per thread)
+    __shared__ int smesh[2];
     if (threadIdx.x == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
@@ -193,13 +199,14 @@ __global__ void __launch_bounds__(32 * kBatchWarps, MINB)
     __syncthreads();
     long long w = blockIdx.x;
     if (threadIdx.x == 0 && w < total)
-        batch_fan_issue<T>(tab, n_meshes, w, cap, bar0, srec0, sslab0);
+        smesh[0] = batch_fan_issue<T>(tab, n_meshes, w, cap, bar0, srec0, sslab0);
+    __syncthreads();
     for (int it = 0; w < total; w += gridDim.x, ++it) {
         const int sg = it & 1;
         const long long wn = w + gridDim.x;
         if (threadIdx.x == 0 && wn < total)
-            batch_fan_issue<T>(tab, n_meshes, wn, cap, bar0 + 8 * (sg ^ 1), stage_rec(srec0, stage_bytes, sg ^ 1), stage_slab(sslab0, stage_bytes, sg ^ 1));
-        const BatchMesh& M = tab[batch_mesh_of(tab, n_meshes, w, true)];
+            smesh[sg ^ 1] = batch_fan_issue<T>(tab, n_meshes, wn, cap, bar0 + 8 * (sg ^ 1), stage_rec(srec0, stage_bytes, sg ^ 1), stage_slab(sslab0, stage_bytes, sg ^ 1));
+        const BatchMesh& M = tab[smesh[sg]];
         int cur, prev, nxt;
         batch_roles(M, rot, cur, prev, nxt);
         const long long local = w - M.f_off;

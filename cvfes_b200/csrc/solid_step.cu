@@ -1186,9 +1186,12 @@ struct StepTuning {
 // Defaults from sweeps on the 256x1024 tube with 512 samples (B200), ms/step:
 // FP32 (velocity-state form): persistent fan 2.441 (4 nodes per block), 2.445 (2), 2.562
 // (3), fan 2.606 (2), 2.598 (4), fan with loads two elements ahead 2.637; FP64: fan 5.750,
-// persistent fan 6.088, two ahead 5.981.  2 blocks per SM worth of registers.
+// persistent fan 6.088 (2 nodes per block), two ahead 5.981; on another box with the
+// final kernels, FP64 persistent fan with 4 nodes per block 5.421 against the fan's 5.821
+// (1 sample per thread at 3 blocks' registers: 6.47 to 8.07).  2 blocks per SM worth of
+// registers.
 static StepTuning g_tune32 = {4, 4, 6, 2};
-static StepTuning g_tune64 = {2, 2, 3, 2};
+static StepTuning g_tune64 = {2, 4, 6, 2};
 // L2 prefetch of the fan kernels: distance in nodes (-1: the mesh's bandwidth + 128;
 // 0: off) and parts (bit 0 node rows, bit 1 element coefficient rows; -1: automatic).
 // Sweeps on the 256x1024 tube (bandwidth 257, 512 samples): 256 .. 768 nodes ahead

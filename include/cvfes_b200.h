@@ -85,8 +85,8 @@ typedef struct cvfes_solid_mesh {
                                      calc_ddu, physicsSolverSDampGPUs.cl:398-429) */
 } cvfes_solid_mesh;
 
-/* Step-kernel tuning (the autotuner sets these; defaults: FP32 variant 6, vec 4,
- * 4 nodes per block; FP64 variant 3, vec 2, 2 nodes per block; minb 2).
+/* Step-kernel tuning (the autotuner sets these; defaults: variant 6 with 4 nodes per
+ * block, vec 4 for FP32 and 2 for FP64; minb 2).
  *   precision 32 | 64;  vec: samples per thread (FP32 1|2|4, FP64 1|2);
  *   npb: nodes per block when a warp owns one node (1..8, one warp each);
  *   staged: 0 = slot records, stiffness rows and gathers read through L1;
