@@ -24,8 +24,8 @@ from . import _lib
 STEP_CANDIDATES = {
     32: [(6, 4, 2, 2), (6, 4, 4, 2), (3, 4, 2, 2), (3, 4, 4, 2), (8, 4, 2, 2), (3, 4, 2, 1),
          (1, 4, 4, 2), (3, 2, 2, 3), (5, 4, 2, 1), (0, 4, 8, 1)],
-    64: [(3, 2, 2, 2), (3, 2, 4, 2), (6, 2, 2, 2), (8, 2, 2, 2), (1, 2, 4, 2), (3, 1, 4, 3),
-         (5, 1, 2, 2), (0, 2, 8, 1)],
+    64: [(6, 2, 4, 2), (3, 2, 2, 2), (3, 2, 4, 2), (6, 2, 2, 2), (8, 2, 2, 2), (1, 2, 4, 2),
+         (3, 1, 4, 3), (5, 1, 2, 2), (0, 2, 8, 1)],
 }
 
 
