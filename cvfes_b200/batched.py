@@ -70,7 +70,7 @@ class BatchedSolidSolver:
     def __init__(self, meshes: Sequence, dts: Sequence[float], precision: int = 32,
                  device="cuda:0", vec: Optional[int] = None, grid: int = 0,
                  graph_chunk: int = 48, max_steps: int = 8192, variant: int = 1,
-                 grouped: bool = True, state: str = "auto"):
+                 grouped: bool = True, state: str = "auto", concurrent: bool = True):
         if len(meshes) != len(dts) or not meshes:
             raise ValueError("one dt per mesh")
         if graph_chunk % 6:
@@ -92,6 +92,10 @@ class BatchedSolidSolver:
         self.grid = grid
         self.variant = variant
         self.grouped = grouped
+        # graph chunks of the groups on streams of their own, so that one group's launch
+        # tails overlap the next group's launches (the meshes are independent)
+        self.concurrent = concurrent
+        self._group_streams: List[torch.cuda.Stream] = []
         self.totals = (_lib.C.c_int64 * 3)()
         self.graph_chunk = graph_chunk
         self.rot = 0
@@ -166,9 +170,11 @@ class BatchedSolidSolver:
     def Advance(self, pressures, use_graph: bool = True):
         """Advance every mesh by len(pressures) steps with the shared pressure schedule.
 
-        The groups advance one after another: each graph chunk (or plain run) takes
-        one group through the same steps, with its own device clock indexing the
-        shared schedule, before the next group's chunk."""
+        Each graph chunk (or plain run) takes one group through the same steps, with its
+        own device clock indexing the shared schedule.  With ``concurrent`` the groups'
+        graph chunks run on streams of their own, joined to the caller's stream before
+        the call returns; otherwise one group's chunk after another on the caller's
+        stream.  Either way every mesh takes its own steps in order."""
         p = np.ascontiguousarray(pressures, dtype=np.float64).ravel()
         n = p.size
         if n > self._p.numel():
@@ -186,15 +192,35 @@ class BatchedSolidSolver:
                     self._plain(lead)
                     done += lead
                 graphs = [self._graph(g, chunk) for g in self.groups]
-                while n - done >= chunk:
-                    for h in graphs:
-                        call("cvfes_graph_launch", h, self._stream())
-                    done += chunk
+                n_chunks = (n - done) // chunk
+                if self.concurrent and len(graphs) > 1:
+                    self._launch_concurrent(graphs, n_chunks)
+                else:
+                    for _ in range(n_chunks):
+                        for h in graphs:
+                            call("cvfes_graph_launch", h, self._stream())
+                done += n_chunks * chunk
             if n - done:
                 self._plain(n - done)
         self.steps += n
         self.sync_roles()
         return self
+
+    def _launch_concurrent(self, graphs, n_chunks):
+        """n_chunks replays of each group's graph on the group's own stream, after the
+        caller's stream's work so far, and the caller's stream waits for all of them."""
+        main = torch.cuda.current_stream(self.device)
+        while len(self._group_streams) < len(graphs):
+            self._group_streams.append(torch.cuda.Stream(device=self.device))
+        start = torch.cuda.Event()
+        start.record(main)
+        for h, st in zip(graphs, self._group_streams):
+            st.wait_event(start)
+            for _ in range(n_chunks):
+                call("cvfes_graph_launch", h, st.cuda_stream)
+            end = torch.cuda.Event()
+            end.record(st)
+            main.wait_event(end)
 
     def sync_roles(self):
         """Set each mesh solver's buffer roles from the batch's rotation phase

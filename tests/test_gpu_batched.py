@@ -33,15 +33,17 @@ class _Cfg:
 
 
 @pytest.mark.parametrize("precision", [32, 64])
-@pytest.mark.parametrize("variant,grouped", [(0, True), (1, True), (1, False)])
-def test_batch_equals_meshes_advanced_alone(lib, cuda, precision, variant, grouped):
+@pytest.mark.parametrize("variant,grouped,concurrent", [(0, True, True), (1, True, True),
+                                                        (1, True, False), (1, False, True)])
+def test_batch_equals_meshes_advanced_alone(lib, cuda, precision, variant, grouped, concurrent):
     """Row-gather (0) and fan (1) batch kernels, meshes of 16..128 samples (several nodes
-    per warp in the fan layout), one launch per item shape or one for all: the bits of
-    each mesh advanced alone."""
+    per warp in the fan layout), one launch per item shape or one for all, the groups'
+    graph chunks on streams of their own or one after another: the bits of each mesh
+    advanced alone."""
     cases, meshes, dts = small_batch()
     pres = 1.33e5 * np.minimum(np.arange(100) / 100.0, 1.0)
     batch = BatchedSolidSolver(meshes, dts, precision=precision, device=cuda, graph_chunk=24,
-                               variant=variant, grouped=grouped)
+                               variant=variant, grouped=grouped, concurrent=concurrent)
     assert batch.variant == variant
     shapes = {fan_item_nodes(m.nSmp, batch.vec) for m in meshes}
     assert len(batch.groups) == (len(shapes) if grouped else 1)
