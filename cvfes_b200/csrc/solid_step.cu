@@ -462,9 +462,10 @@ __global__ void __launch_bounds__(256, MINB) k_step_fanp(StepArgs<T> A, long lon
 // its nodes' terms to FP64 sums in tensor memory (norms_add), and at its end the block
 // writes one row of partial sums, its warps added in order.  A kernel of its own: the
 // plain step without any tensor-memory instruction is 6% faster (2.30 against 2.44
-// ms/step on the 256x1024 tube, and 7.2 against 8.1 ms for 500 steps of the 64x128 tube).  Every wait is bounded: a wait that gives up sets status bit 0, the block
-// stops after the item (all warps leave the loop together), waits with a bound for the
-// copies it issued, frees its tensor memory and returns.
+// ms/step on the 256x1024 tube, and 7.2 against 8.1 ms for 500 steps of the 64x128
+// tube).  Every wait is bounded: a wait that gives up sets status bit 0, the block stops
+// after the item (all warps leave the loop together), waits with a bound for the copies
+// it issued, frees its tensor memory and returns.
 template <typename T, int V, bool DIFF, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_step_fanp_tm(StepArgs<T> A, long long n_items) {
     extern __shared__ __align__(16) unsigned char smem[];
